@@ -1,0 +1,149 @@
+/*
+ * slipcam_b200.h -- the C ABI of the b200 backend of slipcam's framecor Correlator.
+ *
+ * The reference exposes framecor as a C++ interface (slipcam cxx/framecor.h) bound to Python by
+ * pybind11 (cxx/bindings.cpp). This library is the same correlator on a B200, behind plain C:
+ * plain pointers and sizes, an opaque handle, int status codes. A binding (the reference's
+ * bindings.cpp, or the Python package slipcam_b200.framecor through ctypes) turns the codes into
+ * the reference's exceptions:
+ *
+ *   B200_OK        0   success
+ *   B200_EINVAL    1   std::invalid_argument -> ValueError   (cxx/common.cpp:17, bindings.cpp:44-79)
+ *   B200_ERUNTIME  2   std::runtime_error    -> RuntimeError (cxx/cuda.cu:28-38, bindings.cpp:59)
+ *   B200_ETIMEOUT  3   a bounded device wait gave up         -> RuntimeError
+ *
+ * Messages start with "framecor: " as the reference's do; b200_last_error gives the last one.
+ * One handle is not re-entrant (like one reference Correlator); distinct handles are independent.
+ * Host-pointer calls are synchronous: they return when the outputs are in the caller's arrays.
+ *
+ * Outputs, per (frame, window) pair q = frame * windows + window, windows row-major (down, then
+ * across), exactly the reference layout (cxx/framecor.h:38-43):
+ *   offset[2q], offset[2q+1]  (down, across) motion of the frame, NaN if not valid
+ *   peak[q]                   normalized correlation at the peak
+ *   snr[q]                    squared peak over the mean squared surface around it
+ *   cov[3q .. 3q+2]           covariance of the offsets (down, across, cross)
+ */
+#ifndef SLIPCAM_B200_H
+#define SLIPCAM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define B200_API __attribute__((visibility("default")))
+#else
+#define B200_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B200_OK 0
+#define B200_EINVAL 1
+#define B200_ERUNTIME 2
+#define B200_ETIMEOUT 3
+
+/* gross offsets: none, per frame (n x 2), per window (n x windows x 2); int32 (down, across) */
+#define B200_GROSS_NONE 0
+#define B200_GROSS_FRAME 1
+#define B200_GROSS_WINDOW 2
+
+/* the arithmetic of the transforms */
+#define B200_FORM_AUTO 0   /* the library's choice */
+#define B200_FORM_FFT32 1  /* FP32 FFTs on the CUDA cores */
+
+/* The frames, the grid of reference windows and the correlation parameters.
+ * Replaces framecor::Params (cxx/framecor.h:22-35); same fields, same defaults in the binding
+ * (window 64, search 48, stat_size 21, batch 4096). batch is a hint here: the library picks its
+ * own number of frames per launch. */
+typedef struct b200_params {
+    int height, width;      /* frame size, pixels */
+    int window;             /* W, the size of the square reference windows */
+    int search;             /* R, the half search range: shifts -R..R */
+    int stat_size;          /* the size of the surface patch of the SNR */
+    int batch;              /* hint (the reference's FFT batch) */
+    const int32_t *down;    /* ny first rows of the windows */
+    int ny;
+    const int32_t *across;  /* nx first columns of the windows */
+    int nx;
+} b200_params;
+
+typedef struct b200_handle b200_handle;
+
+/* Validate the parameters (cxx/common.cpp:15-28 checkParams, the same messages), pick the device
+ * and allocate everything. Replaces framecor::makeCuda (cxx/framecor.h:65, cxx/cuda.cu:389-393)
+ * as chosen by bindings.cpp:38-44. On failure *out is NULL and b200_last_error(NULL) says why. */
+B200_API int b200_create(const b200_params *p, int device, b200_handle **out);
+
+/* Free the handle and its device memory (the Correlator's destructor, cxx/framecor.h:48). */
+B200_API int b200_destroy(b200_handle *h);
+
+/* The last error message of a handle, or of the calling thread's last b200_create if h is NULL. */
+B200_API const char *b200_last_error(const b200_handle *h);
+
+/* Set the reference frame, height x width uint8 in host memory, row-major: the zero-mean
+ * reference windows, their norms and their spectra, kept resident on the device.
+ * Replaces Correlator::setReference (cxx/framecor.h:50; bindings.cpp:47-55). */
+B200_API int b200_set_reference(b200_handle *h, const uint8_t *frame);
+
+/* Correlate n frames (n x height x width uint8, host memory) with the reference frame; gross:
+ * NULL (gross_mode B200_GROSS_NONE), n x 2 (B200_GROSS_FRAME) or n x windows x 2
+ * (B200_GROSS_WINDOW) int32 in host memory; outputs in host memory, n x windows (x 2, x 3).
+ * n = 0 is a no-op. B200_ERUNTIME before b200_set_reference.
+ * Replaces Correlator::correlate (cxx/framecor.h:53-54) with the gross handling of
+ * bindings.cpp:64-80 (a per-frame gross gives results identical to the same gross per window). */
+B200_API int b200_correlate(b200_handle *h, const uint8_t *frames, int n, const int32_t *gross,
+                   int gross_mode, float *offset, float *peak, float *snr, float *cov);
+
+/* The same two calls on device memory, stream-ordered on `stream` (a cudaStream_t; NULL for the
+ * legacy default stream), without host synchronization. frame rows are `pitch` bytes apart,
+ * frames pitch * height bytes apart. No counterpart in the reference (its CUDA backend copies
+ * from host memory, cxx/cuda.cu:323-358); for inputs already in device memory. */
+B200_API int b200_set_reference_device(b200_handle *h, const uint8_t *frame, int pitch, void *stream);
+B200_API int b200_correlate_device(b200_handle *h, const uint8_t *frames, int n, int pitch,
+                          const int32_t *gross, int gross_mode, float *offset, float *peak,
+                          float *snr, float *cov, void *stream);
+
+/* As b200_correlate_device, also writing each pair's normalized surface (2R+1) x (2R+1) float32
+ * to surface[q * (2R+1)^2 ...] (zeros for invalid pairs). For tests: the surface is the
+ * reference's normalized buffer of cxx/cpu.cpp:146-160. */
+B200_API int b200_correlate_device_surfaces(b200_handle *h, const uint8_t *frames, int n, int pitch,
+                                   const int32_t *gross, int gross_mode, float *offset, float *peak,
+                                   float *snr, float *cov, float *surface, void *stream);
+
+/* The summed-area tables of n frames on the device (cxx/cpu.cpp:24-42, cxx/cuda.cu:72-110):
+ * sat (uint32, exact modulo 2^32) and sat2 (int64), each n x (height + 1) x (width + 1). */
+B200_API int b200_sat_device(const uint8_t *frames, int n, int height, int width, int pitch, uint32_t *sat,
+                    int64_t *sat2, void *stream);
+
+/* The arithmetic of the transforms, B200_FORM_*; B200_EINVAL for an unknown or unbuilt form. */
+B200_API int b200_set_form(b200_handle *h, int form);
+
+/* The grid shape (Correlator.shape, bindings.cpp:139), the FFT size used for the search windows,
+ * and the number of kernels this handle has launched (a running count). */
+B200_API int b200_info(const b200_handle *h, int *ny, int *nx, int *fft_size, uint64_t *launches);
+
+/* Timing of the correlation kernel: while enabled, every launch of the fused correlation kernel
+ * is bracketed by CUDA events on its own stream; b200_profile_read gives the summed event time
+ * (ms), the number of launches and the pairs they processed, and resets the sums. For
+ * measurement; no counterpart in the reference. */
+B200_API int b200_profile(b200_handle *h, int enable);
+B200_API int b200_profile_read(b200_handle *h, double *kernel_ms, uint64_t *kernel_launches,
+                               uint64_t *pairs);
+
+/* "b200" (Correlator.backend, cxx/framecor.h:55). */
+B200_API const char *b200_backend(const b200_handle *h);
+
+/* Whether a CUDA device of compute capability 10.0 is present (framecor::hasCuda,
+ * cxx/framecor.h:63, cxx/cuda.cu:383-387). */
+B200_API int b200_has_device(void);
+
+/* The library version (the module's __version__, bindings.cpp:114). */
+B200_API const char *b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SLIPCAM_B200_H */

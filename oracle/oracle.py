@@ -1,0 +1,179 @@
+"""
+TEST INFRASTRUCTURE: Python access to the oracle. Imported only by tests/, __graft_entry__.smoke()
+and bench.py's CPU leg, as the checker; the product never imports it.
+
+Two oracles:
+
+* ``correlate(...)``: our C restatement of framecor's CPU path (oracle/framecor_oracle.c), in
+  the reference's float arithmetic (``mode='ref32'``) or entirely in double (``mode='f64'``),
+  with the correlation summed directly (no FFT).
+* ``reference_module()``: the reference's own CPU backend and pybind11 module (slipcam
+  cxx/cpu.cpp, cxx/common.cpp, cxx/bindings.cpp), compiled unchanged by oracle/Makefile with the
+  project's FFTW-API shim (oracle/fftw_shim) standing in for FFTW. Its ``Correlator`` has the
+  reference API (bindings.cpp:111-142) with ``backend='cpu'``.
+
+Both are built by ``make -C oracle`` (``build()`` in __graft_entry__.py runs it).
+"""
+
+import ctypes
+import importlib.machinery
+import importlib.util
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, 'liboracle.so')
+REF_DIR = os.path.join(HERE, '_ref')
+
+MODES = {'ref32': 0, 'f64': 1}
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [('height', ctypes.c_int), ('width', ctypes.c_int), ('window', ctypes.c_int),
+                ('search', ctypes.c_int), ('stat_size', ctypes.c_int),
+                ('down', ctypes.POINTER(ctypes.c_int)), ('ny', ctypes.c_int),
+                ('across', ctypes.POINTER(ctypes.c_int)), ('nx', ctypes.c_int)]
+
+
+_lib = None
+
+
+def build():
+    """Compile the oracle library (and the reference module when its sources are present)."""
+    targets = ['oracle']
+    if os.path.isdir('/root/reference/cxx'):
+        targets.append('ref')
+    subprocess.run(['make', '-s', '-C', HERE, *targets], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(LIB_PATH)
+        _lib.orc_correlate.restype = ctypes.c_int
+        _lib.orc_correlate.argtypes = [ctypes.POINTER(_Params), ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        _lib.orc_sat.restype = None
+        _lib.orc_sat.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                 ctypes.c_void_p]
+        _lib.orc_reference_windows.restype = ctypes.c_int
+        _lib.orc_reference_windows.argtypes = [ctypes.POINTER(_Params), ctypes.c_void_p,
+                                               ctypes.c_void_p, ctypes.c_void_p]
+    return _lib
+
+
+def window_grid(height, width, window, search, skip, margin=0):
+    """The grid of windows, restated from python/slipcam/framecor/__init__.py:18-32."""
+    axes = []
+    for size in (height, width):
+        first = margin + search
+        count = (size - margin - search - first - window) // skip
+        if count <= 0:
+            raise ValueError('window_grid: no window fits')
+        axes.append(first + skip * np.arange(count))
+    return tuple(axes)
+
+
+def _params(height, width, down, across, window, search, stat_size):
+    down = np.ascontiguousarray(down, np.int32)
+    across = np.ascontiguousarray(across, np.int32)
+    p = _Params(height, width, window, search, stat_size,
+                down.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(down),
+                across.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(across))
+    return p, (down, across)
+
+
+def expand_gross(gross, n, ny, nx):
+    """Per-pair gross offsets (n, ny, nx, 2) int32 from (n, 2) or (n, ny, nx, 2), as
+    cxx/bindings.cpp:64-80 expands them."""
+    if gross is None:
+        return None
+    g = np.asarray(gross, np.int32)
+    if g.shape == (n, 2):
+        return np.ascontiguousarray(np.broadcast_to(g[:, None, None, :], (n, ny, nx, 2)))
+    if g.shape == (n, ny, nx, 2):
+        return np.ascontiguousarray(g)
+    raise ValueError('gross must be frames x 2 or frames x down x across x 2')
+
+
+def sat(frame):
+    """The exact int64 summed-area tables (h+1, w+1) of a uint8 frame and of its squares."""
+    frame = np.ascontiguousarray(frame, np.uint8)
+    h, w = frame.shape
+    s = np.empty((h + 1, w + 1), np.int64)
+    s2 = np.empty((h + 1, w + 1), np.int64)
+    lib().orc_sat(frame.ctypes.data, h, w, s.ctypes.data, s2.ctypes.data)
+    return s, s2
+
+
+def reference_windows(height, width, down, across, window, reference):
+    """The zero-mean reference windows (nwin, W, W) float32 and their norms (nwin,) float32."""
+    p, keep = _params(height, width, down, across, window, 1, 21)
+    ref = np.ascontiguousarray(reference, np.uint8)
+    nwin = len(down) * len(across)
+    win = np.empty((nwin, window, window), np.float32)
+    norms = np.empty(nwin, np.float32)
+    lib().orc_reference_windows(ctypes.byref(p), ref.ctypes.data, win.ctypes.data, norms.ctypes.data)
+    return win, norms
+
+
+def correlate(height, width, down, across, reference, frames, gross=None, *, window=64, search=48,
+              stat_size=21, mode='f64', surfaces=False, threads=0):
+    """The outputs of framecor's correlate for the frames, from the C restatement.
+
+    Returns a dict like the reference's (offsets, peak, snr, cov, float32, shaped
+    (n, ny, nx, ...)), plus 'offsets64' (float64) and, if surfaces, 'surface' (n, ny, nx, M, M)
+    float64 normalized surfaces.
+    """
+    frames = np.ascontiguousarray(frames, np.uint8)
+    n = frames.shape[0]
+    ny, nx = len(down), len(across)
+    p, keep = _params(height, width, down, across, window, search, stat_size)
+    g = expand_gross(gross, n, ny, nx)
+    ref = np.ascontiguousarray(reference, np.uint8)
+    M = 2 * search + 1
+    out = dict(offsets=np.empty((n, ny, nx, 2), np.float32), peak=np.empty((n, ny, nx), np.float32),
+               snr=np.empty((n, ny, nx), np.float32), cov=np.empty((n, ny, nx, 3), np.float32),
+               offsets64=np.empty((n, ny, nx, 2), np.float64))
+    surf = np.empty((n, ny, nx, M, M), np.float64) if surfaces else None
+    rc = lib().orc_correlate(ctypes.byref(p), ref.ctypes.data, frames.ctypes.data, n,
+                             None if g is None else g.ctypes.data, MODES[mode],
+                             out['offsets'].ctypes.data, out['peak'].ctypes.data,
+                             out['snr'].ctypes.data, out['cov'].ctypes.data,
+                             out['offsets64'].ctypes.data, None if surf is None else surf.ctypes.data,
+                             threads)
+    if rc != 0:
+        raise ValueError(f'oracle: invalid parameters ({rc})')
+    if surfaces:
+        out['surface'] = surf
+    return out
+
+
+_ref_module = None
+
+
+def reference_module():
+    """The reference's pybind11 module _framecor (CPU backend, FFT by the shim), from
+    oracle/_ref; None if it was not built."""
+    global _ref_module
+    if _ref_module is None:
+        if not os.path.isdir(REF_DIR):
+            return None
+        names = [f for f in os.listdir(REF_DIR) if f.startswith('_framecor') and f.endswith('.so')]
+        if not names:
+            return None
+        path = os.path.join(REF_DIR, names[0])
+        loader = importlib.machinery.ExtensionFileLoader('_framecor', path)
+        spec = importlib.util.spec_from_file_location('_framecor', path, loader=loader)
+        mod = importlib.util.module_from_spec(spec)
+        loader.exec_module(mod)
+        sys.modules.setdefault('_oracle_ref_framecor', mod)
+        _ref_module = mod
+    return _ref_module

@@ -1,0 +1,618 @@
+// capi.cu -- the C ABI of include/slipcam_b200.h: the handle, parameter checks, device memory,
+// the launch sequence and the host <-> device streaming.
+//
+// The reference's CUDA backend (slipcam cxx/cuda.cu:249-379) copies a group of frames, builds the
+// tables, then runs six kernels and two cuFFT calls per batch of pairs, synchronously. Here a group
+// of frames is three launches (summed-area tables in two passes, variance denominators) plus one
+// fused correlation launch, and the host path double-buffers groups over two streams: while the
+// device correlates group g, the copy stream brings group g + 1 in and the host stages group g + 2.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/slipcam_b200.h"
+#include "corr_fft.cuh"
+#include "sat.cuh"
+
+using namespace b200;
+
+namespace {
+
+constexpr int kThreads = 256;   // threads per correlation CTA
+thread_local std::string g_create_error;
+
+struct Failure {
+    int code;
+    std::string msg;
+};
+
+[[noreturn]] void fail(int code, const std::string &msg) { throw Failure{code, "framecor: " + msg}; }
+
+void check(cudaError_t e, const char *what)
+{
+    if (e != cudaSuccess) fail(B200_ERUNTIME, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(call) check((call), #call)
+
+// the FFT sizes with a compiled kernel: N = 16 N2 for the radices of dft.cuh
+constexpr int kSizes[] = {16, 32, 48, 64, 80, 96, 128, 144, 160, 192};
+
+int fft_size(int L)
+{
+    for (int n : kSizes)
+        if (n >= L) return n;
+    return 0;
+}
+
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count)
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = count;
+        CK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    }
+    ~DevBuf()
+    {
+        if (p) cudaFree(p);
+    }
+};
+
+template <class T>
+struct HostBuf {
+    T *p = nullptr;
+    void alloc(size_t count)
+    {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        CK(cudaMallocHost(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    }
+    ~HostBuf()
+    {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+// the per-group scratch of one slot
+struct Slot {
+    DevBuf<uint8_t> frames;
+    DevBuf<uint32_t> sat;
+    DevBuf<int64_t> sat2;
+    DevBuf<float> dinv;
+    DevBuf<int32_t> gross;
+    DevBuf<float> out;          // offset 2P | peak P | snr P | cov 3P, P = group * nwin
+    HostBuf<uint8_t> hframes;
+    HostBuf<int32_t> hgross;
+    HostBuf<float> hout;
+    cudaEvent_t in = nullptr, done = nullptr;
+    ~Slot()
+    {
+        if (in) cudaEventDestroy(in);
+        if (done) cudaEventDestroy(done);
+    }
+};
+
+// launch attributes set once per kernel instance
+template <int N>
+void prepare()
+{
+    static bool done[64] = {};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && done[dev]) return;
+    CK(cudaFuncSetAttribute(corr_kernel<N, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(Geo<N>::smem_bytes)));
+    CK(cudaFuncSetAttribute(spectra_kernel<N, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(Geo<N>::smem_bytes)));
+    if (dev >= 0 && dev < 64) done[dev] = true;
+}
+
+template <int N>
+void launch_corr(const CorrArgs &a, cudaStream_t s)
+{
+    prepare<N>();
+    corr_kernel<N, kThreads><<<unsigned(a.nwin) * a.nf, kThreads, Geo<N>::smem_bytes, s>>>(a);
+}
+
+template <int N>
+void launch_spectra(const SpectraArgs &a, int nwin, cudaStream_t s)
+{
+    prepare<N>();
+    spectra_kernel<N, kThreads><<<unsigned(nwin), kThreads, Geo<N>::smem_bytes, s>>>(a);
+}
+
+#define B200_DISPATCH(N_, F, ...)                                                                  \
+    switch (N_) {                                                                                   \
+    case 16: F<16>(__VA_ARGS__); break;                                                             \
+    case 32: F<32>(__VA_ARGS__); break;                                                             \
+    case 48: F<48>(__VA_ARGS__); break;                                                             \
+    case 64: F<64>(__VA_ARGS__); break;                                                             \
+    case 80: F<80>(__VA_ARGS__); break;                                                             \
+    case 96: F<96>(__VA_ARGS__); break;                                                             \
+    case 128: F<128>(__VA_ARGS__); break;                                                           \
+    case 144: F<144>(__VA_ARGS__); break;                                                           \
+    case 160: F<160>(__VA_ARGS__); break;                                                           \
+    case 192: F<192>(__VA_ARGS__); break;                                                           \
+    default: fail(B200_EINVAL, "no kernel for the FFT size " + std::to_string(N_));               \
+    }
+
+void launch_sat(const uint8_t *frames, int64_t fstride, int pitch, int nf, int h, int w, uint32_t *sat,
+                int64_t *sat2, cudaStream_t s)
+{
+    const int64_t sfs = int64_t(h + 1) * (w + 1);
+    sat_rows_kernel<<<dim3(unsigned((h + 7) / 8), unsigned(nf)), 256, 0, s>>>(frames, fstride, pitch, h, w, sat, sat2, sfs);
+    sat_cols_kernel<<<dim3(unsigned((w + 1 + 31) / 32), unsigned(nf)), dim3(32, 8), 0, s>>>(h, w, sat, sat2, sfs);
+}
+
+}   // namespace
+
+struct b200_handle {
+    int height = 0, width = 0, W = 0, R = 0, stat = 21, batch = 4096;
+    std::vector<int> down, across;
+    int ny = 0, nx = 0, nwin = 0, L = 0, M = 0, N = 0;
+    int device = 0;
+    int group = 1;
+    int form = B200_FORM_FFT32;
+    bool ready = false;
+    uint64_t launches = 0;
+    std::string err;
+    cudaStream_t comp = nullptr, copy = nullptr;
+    DevBuf<int> d_down, d_across;
+    DevBuf<float> d_norm;
+    DevBuf<float2> d_spec, d_tw;
+    DevBuf<uint8_t> d_ref;
+    DevBuf<uint32_t> d_sat;      // device-path scratch
+    DevBuf<int64_t> d_sat2;
+    DevBuf<float> d_dinv;
+    Slot slot[2];
+    int fpitch = 0;              // the pitch of the staged frames (a multiple of 16)
+    bool profiling = false;      // events around the correlation launches
+    struct Timed {
+        cudaEvent_t a, b;
+        uint64_t pairs;
+    };
+    std::vector<Timed> timed;
+
+    ~b200_handle()
+    {
+        for (Timed &t : timed) {
+            cudaEventDestroy(t.a);
+            cudaEventDestroy(t.b);
+        }
+        if (comp) cudaStreamDestroy(comp);
+        if (copy) cudaStreamDestroy(copy);
+    }
+
+    int64_t sat_size() const { return int64_t(height + 1) * (width + 1); }
+    int64_t pixels() const { return int64_t(height) * width; }
+
+    // the tables and the correlation of nf frames (device memory) on stream s
+    void run_group(const uint8_t *frames, int pitch, int nf, const int32_t *gross, int gross_mode,
+                   uint32_t *sat, int64_t *sat2, float *dinv, float *offset, float *peak, float *snr,
+                   float *cov, float *surface, cudaStream_t s)
+    {
+        const int64_t fstride = int64_t(pitch) * height;
+        launch_sat(frames, fstride, pitch, nf, height, width, sat, sat2, s);
+        dinv_kernel<<<dim3(unsigned((width - W + 1 + 127) / 128), unsigned(height - W + 1), unsigned(nf)), 128, 0, s>>>(
+            sat, sat2, sat_size(), height, width, W, dinv, pixels());
+        CorrArgs a{};
+        a.frames = frames;
+        a.fstride = fstride;
+        a.pitch = pitch;
+        a.sat = sat;
+        a.sat_fstride = sat_size();
+        a.dinv = dinv;
+        a.dinv_fstride = pixels();
+        a.h = height;
+        a.w = width;
+        a.W = W;
+        a.R = R;
+        a.L = L;
+        a.M = M;
+        a.nx = nx;
+        a.nwin = nwin;
+        a.nf = nf;
+        a.stat = stat;
+        a.down = d_down.p;
+        a.across = d_across.p;
+        a.norm = d_norm.p;
+        a.spec = d_spec.p;
+        a.twiddles = d_tw.p;
+        a.gross = gross;
+        a.gross_mode = gross_mode;
+        a.offset = offset;
+        a.peak = peak;
+        a.snr = snr;
+        a.cov = cov;
+        a.surface = surface;
+        Timed t{};
+        if (profiling) {
+            CK(cudaEventCreate(&t.a));
+            CK(cudaEventCreate(&t.b));
+            t.pairs = uint64_t(nf) * nwin;
+            CK(cudaEventRecord(t.a, s));
+        }
+        B200_DISPATCH(N, launch_corr, a, s);
+        CK(cudaGetLastError());
+        if (profiling) {
+            CK(cudaEventRecord(t.b, s));
+            timed.push_back(t);
+        }
+        launches += 4;
+    }
+};
+
+namespace {
+
+// the twiddle tables of the N-point transform: TW[k1 * N2 + n2] = TWI[n2 * 16 + k1] = w_N^{n2 k1}
+std::vector<float2> twiddles(int N)
+{
+    const int N2 = N / 16;
+    std::vector<float2> t(2 * size_t(N));
+    for (int k1 = 0; k1 < 16; ++k1)
+        for (int n2 = 0; n2 < N2; ++n2) {
+            double c = 0.0, s = 0.0;
+            cs2pi(long(n2) * k1, N, c, s);
+            const float2 w = make_float2(float(c), float(-s));
+            t[k1 * N2 + n2] = w;
+            t[N + n2 * 16 + k1] = w;
+        }
+    return t;
+}
+
+// checkParams (cxx/common.cpp:15-28), the same conditions and messages
+void check_params(const b200_params *p)
+{
+    if (!p) fail(B200_EINVAL, "no parameters");
+    if (p->height <= 0 || p->width <= 0) fail(B200_EINVAL, "the frame size must be positive");
+    if (p->window < 3) fail(B200_EINVAL, "the window must be at least 3 pixels");
+    if (p->search < 1) fail(B200_EINVAL, "the half search range must be at least 1 pixel");
+    if (p->ny <= 0 || p->nx <= 0 || !p->down || !p->across) fail(B200_EINVAL, "no windows");
+    for (int i = 0; i < p->ny; ++i)
+        if (p->down[i] < 0 || p->down[i] + p->window > p->height)
+            fail(B200_EINVAL, "a window is outside the frame (down " + std::to_string(p->down[i]) + ")");
+    for (int i = 0; i < p->nx; ++i)
+        if (p->across[i] < 0 || p->across[i] + p->window > p->width)
+            fail(B200_EINVAL, "a window is outside the frame (across " + std::to_string(p->across[i]) + ")");
+    if (p->stat_size < 3) fail(B200_EINVAL, "the SNR window must be at least 3 pixels");
+    if (p->batch < 1) fail(B200_EINVAL, "the batch must be at least 1 window");
+}
+
+template <class F>
+int guarded(b200_handle *h, F &&f)
+{
+    if (!h) return B200_EINVAL;
+    try {
+        f();
+        h->err.clear();
+        return B200_OK;
+    } catch (const Failure &e) {
+        h->err = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        h->err = "framecor: out of host memory";
+        return B200_ERUNTIME;
+    } catch (const std::exception &e) {
+        h->err = std::string("framecor: ") + e.what();
+        return B200_ERUNTIME;
+    }
+}
+
+void upload_reference(b200_handle *h, const uint8_t *dframe, int pitch, cudaStream_t s)
+{
+    SpectraArgs a{};
+    a.frame = dframe;
+    a.pitch = pitch;
+    a.W = h->W;
+    a.nx = h->nx;
+    a.down = h->d_down.p;
+    a.across = h->d_across.p;
+    a.norm = h->d_norm.p;
+    a.spec = h->d_spec.p;
+    a.twiddles = h->d_tw.p;
+    B200_DISPATCH(h->N, launch_spectra, a, h->nwin, s);
+    CK(cudaGetLastError());
+    h->launches += 1;
+}
+
+}   // namespace
+
+extern "C" {
+
+int b200_create(const b200_params *p, int device, b200_handle **out)
+{
+    if (out) *out = nullptr;
+    b200_handle *h = nullptr;
+    try {
+        if (!out) fail(B200_EINVAL, "no output handle");
+        check_params(p);
+        const int L = p->window + 2 * p->search;
+        const int N = fft_size(L);
+        if (!N)
+            fail(B200_EINVAL, "the search window (window + 2 search = " + std::to_string(L)
+                                  + ") is larger than the b200 backend's largest transform, 192");
+        h = new b200_handle;
+        h->height = p->height;
+        h->width = p->width;
+        h->W = p->window;
+        h->R = p->search;
+        h->stat = p->stat_size;
+        h->batch = p->batch;
+        h->down.assign(p->down, p->down + p->ny);
+        h->across.assign(p->across, p->across + p->nx);
+        h->ny = p->ny;
+        h->nx = p->nx;
+        h->nwin = p->ny * p->nx;
+        h->L = L;
+        h->M = 2 * p->search + 1;
+        h->N = N;
+        h->device = device;
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count <= device || device < 0)
+            fail(B200_ERUNTIME, "no CUDA device " + std::to_string(device));
+        CK(cudaSetDevice(device));
+        CK(cudaStreamCreateWithFlags(&h->comp, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking));
+        // frames per launch: enough pairs to fill the GPU many times over, at most 32 frames
+        h->group = std::clamp((32768 + h->nwin - 1) / h->nwin, 1, 32);
+        h->fpitch = (h->width + 15) & ~15;
+        h->d_down.alloc(h->ny);
+        h->d_across.alloc(h->nx);
+        CK(cudaMemcpy(h->d_down.p, h->down.data(), h->ny * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->d_across.p, h->across.data(), h->nx * sizeof(int), cudaMemcpyHostToDevice));
+        h->d_norm.alloc(h->nwin);
+        h->d_spec.alloc(size_t(h->nwin) * (N / 2 + 1) * N);
+        const std::vector<float2> tw = twiddles(N);
+        h->d_tw.alloc(tw.size());
+        CK(cudaMemcpy(h->d_tw.p, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice));
+        h->d_ref.alloc(size_t(h->height) * h->fpitch);
+        const size_t G = size_t(h->group), P = G * h->nwin;
+        h->d_sat.alloc(G * h->sat_size());
+        h->d_sat2.alloc(G * h->sat_size());
+        h->d_dinv.alloc(G * h->pixels());
+        for (Slot &s : h->slot) {
+            s.frames.alloc(G * h->height * h->fpitch);
+            s.sat.alloc(G * h->sat_size());
+            s.sat2.alloc(G * h->sat_size());
+            s.dinv.alloc(G * h->pixels());
+            s.gross.alloc(2 * P);
+            s.out.alloc(7 * P);
+            s.hframes.alloc(G * h->height * h->fpitch);
+            s.hgross.alloc(2 * P);
+            s.hout.alloc(7 * P);
+            CK(cudaEventCreateWithFlags(&s.in, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+        }
+        *out = h;
+        g_create_error.clear();
+        return B200_OK;
+    } catch (const Failure &e) {
+        delete h;
+        g_create_error = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        delete h;
+        g_create_error = "framecor: out of host memory";
+        return B200_ERUNTIME;
+    }
+}
+
+int b200_destroy(b200_handle *h)
+{
+    if (!h) return B200_OK;
+    cudaSetDevice(h->device);
+    if (h->comp) cudaStreamSynchronize(h->comp);
+    if (h->copy) cudaStreamSynchronize(h->copy);
+    delete h;
+    return B200_OK;
+}
+
+const char *b200_last_error(const b200_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int b200_set_form(b200_handle *h, int form)
+{
+    return guarded(h, [&] {
+        if (form != B200_FORM_AUTO && form != B200_FORM_FFT32) fail(B200_EINVAL, "unknown form " + std::to_string(form));
+        h->form = B200_FORM_FFT32;
+    });
+}
+
+int b200_set_reference(b200_handle *h, const uint8_t *frame)
+{
+    return guarded(h, [&] {
+        if (!frame) fail(B200_EINVAL, "no reference frame");
+        CK(cudaSetDevice(h->device));
+        CK(cudaMemcpy2DAsync(h->d_ref.p, h->fpitch, frame, h->width, h->width, h->height, cudaMemcpyHostToDevice, h->comp));
+        upload_reference(h, h->d_ref.p, h->fpitch, h->comp);
+        CK(cudaStreamSynchronize(h->comp));
+        h->ready = true;
+    });
+}
+
+int b200_set_reference_device(b200_handle *h, const uint8_t *frame, int pitch, void *stream)
+{
+    return guarded(h, [&] {
+        if (!frame || pitch < h->width) fail(B200_EINVAL, "no reference frame, or its pitch is below its width");
+        CK(cudaSetDevice(h->device));
+        upload_reference(h, frame, pitch, static_cast<cudaStream_t>(stream));
+        h->ready = true;
+    });
+}
+
+int b200_correlate(b200_handle *h, const uint8_t *frames, int n, const int32_t *gross, int gross_mode,
+                   float *offset, float *peak, float *snr, float *cov)
+{
+    return guarded(h, [&] {
+        if (!h->ready) fail(B200_ERUNTIME, "set_reference first");
+        if (n < 0) fail(B200_EINVAL, "the number of frames must not be negative");
+        if (gross_mode < B200_GROSS_NONE || gross_mode > B200_GROSS_WINDOW || (gross_mode && !gross))
+            fail(B200_EINVAL, "gross must be frames x 2 or frames x down x across x 2");
+        if (n == 0) return;
+        if (!frames || !offset || !peak || !snr || !cov) fail(B200_EINVAL, "null input or output");
+        CK(cudaSetDevice(h->device));
+        const int G = h->group, nwin = h->nwin;
+        const size_t frame_bytes = size_t(h->height) * h->width;
+        const int ngroups = (n + G - 1) / G;
+        // frames in page-locked memory are copied to the device directly, others staged
+        cudaPointerAttributes attr{};
+        const bool pinned = cudaPointerGetAttributes(&attr, frames) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        auto drain = [&](int g) {   // the outputs of group g to the caller's arrays
+            Slot &s = h->slot[g % 2];
+            CK(cudaEventSynchronize(s.done));
+            const int f0 = g * G, nf = std::min(G, n - f0);
+            const size_t P = size_t(nf) * nwin, PG = size_t(G) * nwin, q0 = size_t(f0) * nwin;
+            std::memcpy(offset + 2 * q0, s.hout.p, 2 * P * sizeof(float));
+            std::memcpy(peak + q0, s.hout.p + 2 * PG, P * sizeof(float));
+            std::memcpy(snr + q0, s.hout.p + 3 * PG, P * sizeof(float));
+            std::memcpy(cov + 3 * q0, s.hout.p + 4 * PG, 3 * P * sizeof(float));
+        };
+        for (int g = 0; g < ngroups; ++g) {
+            Slot &s = h->slot[g % 2];
+            if (g >= 2) drain(g - 2);   // also: group g - 2 no longer needs this slot's buffers
+            const int f0 = g * G, nf = std::min(G, n - f0);
+            const size_t P = size_t(nf) * nwin, PG = size_t(G) * nwin;
+            const uint8_t *src = frames + f0 * frame_bytes;
+            if (!pinned) {
+                std::memcpy(s.hframes.p, src, nf * frame_bytes);
+                src = s.hframes.p;
+            }
+            const int32_t *dg = nullptr;
+            size_t gbytes = 0;
+            if (gross_mode == B200_GROSS_FRAME) {
+                gbytes = size_t(nf) * 2 * sizeof(int32_t);
+                std::memcpy(s.hgross.p, gross + 2 * size_t(f0), gbytes);
+            } else if (gross_mode == B200_GROSS_WINDOW) {
+                gbytes = P * 2 * sizeof(int32_t);
+                std::memcpy(s.hgross.p, gross + 2 * size_t(f0) * nwin, gbytes);
+            }
+            CK(cudaMemcpy2DAsync(s.frames.p, h->fpitch, src, h->width, h->width, size_t(nf) * h->height,
+                                 cudaMemcpyHostToDevice, h->copy));
+            if (gbytes) {
+                CK(cudaMemcpyAsync(s.gross.p, s.hgross.p, gbytes, cudaMemcpyHostToDevice, h->copy));
+                dg = s.gross.p;
+            }
+            CK(cudaEventRecord(s.in, h->copy));
+            CK(cudaStreamWaitEvent(h->comp, s.in, 0));
+            float *o = s.out.p;
+            h->run_group(s.frames.p, h->fpitch, nf, dg, gross_mode, s.sat.p, s.sat2.p, s.dinv.p, o, o + 2 * PG,
+                         o + 3 * PG, o + 4 * PG, nullptr, h->comp);
+            CK(cudaMemcpyAsync(s.hout.p, s.out.p, 7 * PG * sizeof(float), cudaMemcpyDeviceToHost, h->comp));
+            CK(cudaEventRecord(s.done, h->comp));
+        }
+        for (int g = std::max(0, ngroups - 2); g < ngroups; ++g) drain(g);
+    });
+}
+
+static int correlate_device(b200_handle *h, const uint8_t *frames, int n, int pitch, const int32_t *gross,
+                            int gross_mode, float *offset, float *peak, float *snr, float *cov, float *surface,
+                            void *stream)
+{
+    return guarded(h, [&] {
+        if (!h->ready) fail(B200_ERUNTIME, "set_reference first");
+        if (n < 0) fail(B200_EINVAL, "the number of frames must not be negative");
+        if (gross_mode < B200_GROSS_NONE || gross_mode > B200_GROSS_WINDOW || (gross_mode && !gross))
+            fail(B200_EINVAL, "gross must be frames x 2 or frames x down x across x 2");
+        if (n == 0) return;
+        if (!frames || pitch < h->width || !offset || !peak || !snr || !cov) fail(B200_EINVAL, "null input or output, or a pitch below the width");
+        CK(cudaSetDevice(h->device));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const int G = h->group, nwin = h->nwin;
+        const int64_t fstride = int64_t(pitch) * h->height;
+        for (int f0 = 0; f0 < n; f0 += G) {
+            const int nf = std::min(G, n - f0);
+            const size_t q0 = size_t(f0) * nwin;
+            const int32_t *g = gross_mode == B200_GROSS_FRAME ? gross + 2 * size_t(f0)
+                             : gross_mode == B200_GROSS_WINDOW ? gross + 2 * q0 : nullptr;
+            h->run_group(frames + f0 * fstride, pitch, nf, g, gross_mode, h->d_sat.p, h->d_sat2.p, h->d_dinv.p,
+                         offset + 2 * q0, peak + q0, snr + q0, cov + 3 * q0,
+                         surface ? surface + q0 * size_t(h->M) * h->M : nullptr, s);
+        }
+    });
+}
+
+int b200_correlate_device(b200_handle *h, const uint8_t *frames, int n, int pitch, const int32_t *gross,
+                          int gross_mode, float *offset, float *peak, float *snr, float *cov, void *stream)
+{
+    return correlate_device(h, frames, n, pitch, gross, gross_mode, offset, peak, snr, cov, nullptr, stream);
+}
+
+int b200_correlate_device_surfaces(b200_handle *h, const uint8_t *frames, int n, int pitch, const int32_t *gross,
+                                   int gross_mode, float *offset, float *peak, float *snr, float *cov,
+                                   float *surface, void *stream)
+{
+    if (!surface) {
+        if (h) h->err = "framecor: no surface output";
+        return B200_EINVAL;
+    }
+    return correlate_device(h, frames, n, pitch, gross, gross_mode, offset, peak, snr, cov, surface, stream);
+}
+
+int b200_sat_device(const uint8_t *frames, int n, int height, int width, int pitch, uint32_t *sat, int64_t *sat2,
+                    void *stream)
+{
+    if (n < 0 || height <= 0 || width <= 0 || pitch < width || (n && (!frames || !sat || !sat2))) return B200_EINVAL;
+    if (n == 0) return B200_OK;
+    launch_sat(frames, int64_t(pitch) * height, pitch, n, height, width, sat, sat2, static_cast<cudaStream_t>(stream));
+    return cudaGetLastError() == cudaSuccess ? B200_OK : B200_ERUNTIME;
+}
+
+int b200_profile(b200_handle *h, int enable)
+{
+    return guarded(h, [&] { h->profiling = enable != 0; });
+}
+
+int b200_profile_read(b200_handle *h, double *kernel_ms, uint64_t *kernel_launches, uint64_t *pairs)
+{
+    return guarded(h, [&] {
+        double ms = 0.0;
+        uint64_t np = 0;
+        for (auto &t : h->timed) {
+            CK(cudaEventSynchronize(t.b));
+            float e = 0.f;
+            CK(cudaEventElapsedTime(&e, t.a, t.b));
+            ms += e;
+            np += t.pairs;
+            cudaEventDestroy(t.a);
+            cudaEventDestroy(t.b);
+        }
+        if (kernel_ms) *kernel_ms = ms;
+        if (kernel_launches) *kernel_launches = h->timed.size();
+        if (pairs) *pairs = np;
+        h->timed.clear();
+    });
+}
+
+int b200_info(const b200_handle *h, int *ny, int *nx, int *fft_size, uint64_t *launches)
+{
+    if (!h) return B200_EINVAL;
+    if (ny) *ny = h->ny;
+    if (nx) *nx = h->nx;
+    if (fft_size) *fft_size = h->N;
+    if (launches) *launches = h->launches;
+    return B200_OK;
+}
+
+const char *b200_backend(const b200_handle *) { return "b200"; }
+
+int b200_has_device(void)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) return 0;
+    for (int d = 0; d < count; ++d) {
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, d) == cudaSuccess && prop.major == 10) return 1;
+    }
+    return 0;
+}
+
+const char *b200_version(void) { return "0.1.0"; }
+
+}   // extern "C"
