@@ -90,6 +90,19 @@ class Clocks:
                 'samples': len(sm)}
 
 
+def profiled_traffic(form, fft_n):
+    """dram bytes per launch of the correlation kernel from the committed ncu summary of this
+    workload (profiles/corr_<form>_720p_w64_s48.md), or None"""
+    path = os.path.join(ROOT, 'profiles', f'corr_{form}_720p_w64_s48.md')
+    try:
+        for line in open(path):
+            if line.startswith('dram_bytes_per_launch:'):
+                return int(line.split(':')[1])
+    except OSError:
+        pass
+    return None
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
@@ -175,12 +188,13 @@ def run_b200(args):
     from slipcam_b200 import framecor, synth
     down, across = framecor.window_grid(H, W_, WIN, SEARCH, SKIP)
     nwin = len(down) * len(across)
-    frames, motion, step, gross = synth.hd(n=NFRAMES, device='cuda')
+    frames, motion, step, gross = synth.hd(n=NFRAMES, device='cuda', count=args.video)
     gross_d = torch.as_tensor(gross).cuda()
     cor = framecor.Correlator(H, W_, down, across, window=WIN, search=SEARCH, backend='b200', device=local)
     cor.set_reference(frames[0])
     fft_n = cor.info()[2]
-    nb = (NFRAMES - 1) // BATCH
+    BATCH = args.batch
+    nb = (len(frames) - 1) // BATCH
     starts = [1 + ((rank + world * i) % nb) * BATCH for i in range(args.warmup + args.steps + 8)]
 
     def step_dev(i):
@@ -217,6 +231,9 @@ def run_b200(args):
         ms = float(t.item())
     value = world * args.steps * BATCH * nwin / (ms / 1e3)
 
+    if args.no_e2e:
+        print(json.dumps({'value': value, 'kernel_ms': kernel_ms, 'kernel_launches': kernel_launches}))
+        return
     # end to end through the host entry point: frames in page-locked memory, numpy outputs
     host = torch.empty(frames.shape, dtype=torch.uint8, pin_memory=True)
     host.copy_(frames)
@@ -275,7 +292,10 @@ def run_b200(args):
                     'd2h_bytes_per_step': BATCH * nwin * 7 * 4},
             'gpu_launches': launches,
             'roofline': {'bound': 'fp32', 'achieved': achieved, 'peak': fp32_peak, 'unit': 'TFLOP/s',
-                         'frac': (achieved / fp32_peak) if achieved else None, 'traffic': None,
+                         'frac': (achieved / fp32_peak) if achieved else None,
+                         'traffic': profiled_traffic('fft32', fft_n) if BATCH == 16 else None,
+                         'traffic_source': 'ncu dram__bytes_read.sum + dram__bytes_write.sum of one 16-frame launch '
+                                           '(profiles/corr_fft32_720p_w64_s48.md)',
                          'kernel': 'corr_kernel<160>', 'kernel_ms_per_launch': kernel_ms / max(kernel_launches, 1),
                          'peak_source': 'nominal FP32 CUDA-core peak: 148 SMs x 128 lanes x 2 x max SM clock',
                          'flop_per_window': fft_flops(fft_n)},
@@ -300,6 +320,9 @@ def main():
     p.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     p.add_argument('--cpu-frames', type=int, default=2)
     p.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline')
+    p.add_argument('--no-e2e', action='store_true', help='device timing only (profiling runs)')
+    p.add_argument('--video', type=int, default=NFRAMES, help='frames of the synthetic video to render')
+    p.add_argument('--batch', type=int, default=BATCH, help='frames per step')
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == 'reference':

@@ -361,7 +361,7 @@ int b200_create(const b200_params *p, int device, b200_handle **out)
         CK(cudaStreamCreateWithFlags(&h->comp, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking));
         // frames per launch: enough pairs to fill the GPU many times over, at most 32 frames
-        h->group = std::clamp((32768 + h->nwin - 1) / h->nwin, 1, 32);
+        h->group = std::clamp((40000 + h->nwin - 1) / h->nwin, 1, 32);
         h->fpitch = (h->width + 15) & ~15;
         h->d_down.alloc(h->ny);
         h->d_across.alloc(h->nx);
@@ -524,7 +524,8 @@ static int correlate_device(b200_handle *h, const uint8_t *frames, int n, int pi
         if (!frames || pitch < h->width || !offset || !peak || !snr || !cov) fail(B200_EINVAL, "null input or output, or a pitch below the width");
         CK(cudaSetDevice(h->device));
         cudaStream_t s = static_cast<cudaStream_t>(stream);
-        const int G = h->group, nwin = h->nwin;
+        // groups of equal size, at most h->group frames
+        const int G = (n + (n + h->group - 1) / h->group - 1) / ((n + h->group - 1) / h->group), nwin = h->nwin;
         const int64_t fstride = int64_t(pitch) * h->height;
         for (int f0 = 0; f0 < n; f0 += G) {
             const int nf = std::min(G, n - f0);

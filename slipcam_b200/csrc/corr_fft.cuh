@@ -204,15 +204,39 @@ __global__ void __launch_bounds__(NT, (N <= 160 ? 2 : 1)) corr_kernel(CorrArgs a
         + sat[sy * ss + sx];
     const float mean = float(box) / (float(L) * float(L));
     const int Lr = (L + 1) & ~1;
-    const uint8_t *src = a.frames + f * a.fstride + int64_t(sy) * a.pitch + sx;
-    for (int idx = threadIdx.x; idx < Lr * N; idx += NT) {
-        const int i = idx / N, j = idx % N;
-        Sr[size_t(i) * G::RP + j] = (i < L && j < L) ? float(src[size_t(i) * a.pitch + j]) - mean : 0.0f;
+    const uint8_t *frame = a.frames + f * a.fstride;
+    int off = 0;
+    if (((a.pitch | reinterpret_cast<uintptr_t>(frame)) & 3) == 0) {
+        // 4-byte words: row i of the chip lands at float column off + j (off = sx mod 4), so every
+        // word, aligned in global memory, is one aligned float4 in shared memory
+        off = sx & 3;
+        constexpr int NW = N / 4 + 1;   // RP = N + 4 floats = NW words per row
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(frame + int64_t(sy) * a.pitch + (sx - off));
+        const int pw = a.pitch >> 2;
+#pragma unroll 4
+        for (int idx = threadIdx.x; idx < Lr * NW; idx += NT) {
+            const int i = idx / NW, w = idx % NW, c0 = 4 * w - off;
+            // a word with a pixel of the chip lies inside the frame row (pitch >= width rounded up to 4)
+            const uint32_t word = (i < L && c0 < L) ? __ldg(src + size_t(i) * pw + w) : 0u;
+            float4 v;
+            v.x = (i < L && c0 >= 0 && c0 < L) ? float(word & 255u) - mean : 0.0f;
+            v.y = (i < L && c0 + 1 >= 0 && c0 + 1 < L) ? float((word >> 8) & 255u) - mean : 0.0f;
+            v.z = (i < L && c0 + 2 >= 0 && c0 + 2 < L) ? float((word >> 16) & 255u) - mean : 0.0f;
+            v.w = (i < L && c0 + 3 < L) ? float(word >> 24) - mean : 0.0f;
+            *reinterpret_cast<float4 *>(Sr + size_t(i) * G::RP + 4 * w) = v;
+        }
+    } else {
+        const uint8_t *src = frame + int64_t(sy) * a.pitch + sx;
+#pragma unroll 4
+        for (int idx = threadIdx.x; idx < Lr * N; idx += NT) {
+            const int i = idx / N, j = idx % N;
+            Sr[size_t(i) * G::RP + j] = (i < L && j < L) ? float(__ldg(src + size_t(i) * a.pitch + j)) - mean : 0.0f;
+        }
     }
     __syncthreads();
 
     const DevExec ex{warp, NT / 32};
-    row_forward<N>(ex, S, Lr / 2, TW);
+    row_forward<N>(ex, S, Lr / 2, TW, off);
     __syncthreads();
     col_pass<N, true>(ex, S, Lr, M, TW, TWI, a.spec + size_t(k) * G::NH * N, nullptr);
     __syncthreads();

@@ -56,9 +56,10 @@ struct HostExec {
     }
 };
 
-// rows [0, 2P) of S hold real rows (floats, pitch RP); on return, their half spectra
+// rows [0, 2P) of S hold real rows (floats, pitch RP, element n of a row at float column
+// off + n, off < 4); on return, their half spectra
 template <int N, class Ex>
-B200_HD void row_forward(const Ex &ex, float2 *S, int P, const float2 *TW)
+B200_HD void row_forward(const Ex &ex, float2 *S, int P, const float2 *TW, int off = 0)
 {
     using G = Geo<N>;
     constexpr int N2 = G::N2, NHP = G::NHP, NU = G::NU, NH = G::NH;
@@ -73,7 +74,7 @@ B200_HD void row_forward(const Ex &ex, float2 *S, int P, const float2 *TW)
                 [&](int lane, St &s) {   // step 1 on the complex row (row 2p) + i (row 2p+1)
                     const int p = 2 * g + (lane & 1), n2 = lane >> 1;
                     if (p < P && n2 < N2) {
-                        const float *xa = reinterpret_cast<const float *>(S + size_t(2 * p) * NHP);
+                        const float *xa = reinterpret_cast<const float *>(S + size_t(2 * p) * NHP) + off;
                         const float *xb = xa + G::RP;
                         fwd_step1<N>(n2, TW, s.y, [&](int n) { return make_float2(xa[n], xb[n]); });
                     }

@@ -24,6 +24,9 @@ torch = pytest.importorskip('torch')
 
 SUPPORTED = [n for n in cases.NAMES if n != 'big']   # window 128 + search 64: L = 256, not yet
 NEAR_TIE = 1e-5
+# the share of integer peaks allowed to differ, each one a verified near-tie; 'mixed' has periodic
+# stripes (8 px) whose surfaces have exactly equal maxima, decided by rounding alone
+TIE_SHARE = {'mixed': 0.2}
 
 
 def golden(name):
@@ -76,7 +79,7 @@ def test_golden(name):
     assert np.all(r['cov'][~valid] == np.array([99, 99, 0], np.float32))
     d = np.abs(a - b).max(-1)
     mism = valid & (d > 0.5)
-    assert mism.sum() <= max(1, valid.sum() // 100), f'{mism.sum()} integer peaks differ'
+    assert mism.sum() <= max(1, int(valid.sum() * TIE_SHARE.get(name, 0.01))), f'{mism.sum()} integer peaks differ'
     assert near_tie_ok(c, mism, r, g, NEAR_TIE)
     ok = valid & ~mism
     assert d[ok].max() < 1e-3, d[ok].max()
@@ -101,7 +104,8 @@ def test_fp64_oracle(name):
     valid = np.isfinite(o['offsets'][..., 0])
     d = np.abs(o['offsets64'] - b['offsets']).max(-1)
     mism = valid & (d > 0.5)
-    assert mism.sum() <= max(1, valid.sum() // 100)
+    assert mism.sum() <= max(1, int(valid.sum() * TIE_SHARE.get(name, 0.01)))
+    assert near_tie_ok(c, mism, b, o, NEAR_TIE) if gross is None or gross.ndim == 2 else True
     ok = valid & ~mism
     assert d[ok].max() < 0.01, d[ok].max()
     assert np.abs(b['snr'][ok] / o['snr'][ok] - 1).max() < 1e-3
