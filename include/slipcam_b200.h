@@ -112,6 +112,18 @@ B200_API int b200_correlate_device_surfaces(b200_handle *h, const uint8_t *frame
                                    const int32_t *gross, int gross_mode, float *offset, float *peak,
                                    float *snr, float *cov, float *surface, void *stream);
 
+/* As b200_correlate_device, for callers that cannot allocate device memory when they
+ * correlate: a capture loop that must never stall on cudaMalloc's implicit synchronization, or a
+ * host that owns all device memory through its own arena. No counterpart in the reference.
+ * The per-frame tables live in one static 32 MiB device array (enough for one 1920 x 1080 frame;
+ * frames go as many per launch as fit), held by every device that loads the library until the
+ * process exits; nothing is allocated. Larger frames are rejected with B200_EINVAL. The first call
+ * on a device looks the array's address up (cudaGetSymbolAddress): make it before any stream
+ * capture. All calls on a device share the array: calls that overlap on the GPU race. */
+B200_API int b200_correlate_device_noalloc(b200_handle *h, const uint8_t *frames, int n, int pitch,
+                                           const int32_t *gross, int gross_mode, float *offset,
+                                           float *peak, float *snr, float *cov, void *stream);
+
 /* The summed-area tables of n frames on the device (cxx/cpu.cpp:24-42, cxx/cuda.cu:72-110):
  * sat (uint32, exact modulo 2^32) and sat2 (int64), each n x (height + 1) x (width + 1). */
 B200_API int b200_sat_device(const uint8_t *frames, int n, int height, int width, int pitch, uint32_t *sat,

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -554,6 +555,122 @@ int b200_correlate_device_surfaces(b200_handle *h, const uint8_t *frames, int n,
         return B200_EINVAL;
     }
     return correlate_device(h, frames, n, pitch, gross, gross_mode, offset, peak, snr, cov, surface, stream);
+}
+
+}   // extern "C"
+
+// ---- the correlation without allocation -------------------------------------------------------
+//
+// Some callers cannot allocate device memory when they correlate: a capture loop that must never
+// stall on cudaMalloc's implicit device synchronization, or a host that owns all device memory
+// through its own arena and forbids the library from taking more. For them,
+// b200_correlate_device_noalloc keeps the per-frame tables (summed-area tables and variance
+// denominators) in one static device array, reserved when the library is loaded on a device and
+// held until the process exits, instead of in buffers of the handle. Nothing here calls cudaMalloc,
+// cudaFree or any allocating routine.
+//
+// The array holds 32 MiB: the tables of one 1920 x 1080 frame (16.0 bytes per pixel). Frames are
+// correlated as many per launch as their tables fit. In host code the array's name is only a
+// stand-in for its device address, so the address is looked up with cudaGetSymbolAddress, once per
+// device, by the first call on that device with the device current; make that first call before
+// any stream capture. Every call on a device shares the array, so calls that overlap on the GPU
+// (two streams, two threads) race on it; keep them ordered. No part of the array has to start at
+// zero: each call writes every table entry it reads (row and column 0 of the summed-area tables
+// included) before the correlation kernel reads it.
+namespace {
+
+constexpr size_t kNoAllocBytes = size_t(32) << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+void *g_noalloc_addr[64] = {};
+std::mutex g_noalloc_mutex;
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+}   // namespace
+
+extern "C" {
+
+int b200_correlate_device_noalloc(b200_handle *h, const uint8_t *frames, int n, int pitch, const int32_t *gross,
+                                  int gross_mode, float *offset, float *peak, float *snr, float *cov, void *stream)
+{
+    return guarded(h, [&] {
+        if (!h->ready) fail(B200_ERUNTIME, "set_reference first");
+        if (n < 0) fail(B200_EINVAL, "the number of frames must not be negative");
+        if (gross_mode < B200_GROSS_NONE || gross_mode > B200_GROSS_WINDOW || (gross_mode && !gross))
+            fail(B200_EINVAL, "gross must be frames x 2 or frames x down x across x 2");
+        if (n == 0) return;
+        if (!frames || pitch < h->width || !offset || !peak || !snr || !cov)
+            fail(B200_EINVAL, "null input or output, or a pitch below the width");
+        // the tables of one frame: 32-bit and 64-bit summed-area tables, variance denominators
+        const size_t b32 = size_t(h->sat_size()) * sizeof(uint32_t), b64 = size_t(h->sat_size()) * sizeof(int64_t);
+        const size_t bd = size_t(h->pixels()) * sizeof(float);
+        const size_t per_frame = align256(b32) + align256(b64) + align256(bd);
+        if (per_frame > kNoAllocBytes)
+            fail(B200_EINVAL, "the frame is too large for the no-allocation entry point: its tables need "
+                                  + std::to_string(per_frame) + " bytes, the static scratch holds "
+                                  + std::to_string(kNoAllocBytes) + " (one 1920 x 1080 frame)");
+        if (h->device < 0 || h->device >= 64) fail(B200_EINVAL, "device index out of range");
+        CK(cudaSetDevice(h->device));
+        void *base = nullptr;
+        {
+            std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+            if (!g_noalloc_addr[h->device]) {
+                void *p = nullptr;
+                CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+                g_noalloc_addr[h->device] = p;
+            }
+            base = g_noalloc_addr[h->device];
+        }
+        const int G = int(std::min<size_t>(kNoAllocBytes / per_frame, size_t(h->group)));
+        unsigned char *q = static_cast<unsigned char *>(base);
+        uint32_t *sat = reinterpret_cast<uint32_t *>(q);
+        int64_t *sat2 = reinterpret_cast<int64_t *>(q + align256(G * b32));
+        float *dinv = reinterpret_cast<float *>(q + align256(G * b32) + align256(G * b64));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const int nwin = h->nwin;
+        const int64_t fstride = int64_t(pitch) * h->height;
+        for (int f0 = 0; f0 < n; f0 += G) {
+            const int nf = std::min(G, n - f0);
+            const size_t q0 = size_t(f0) * nwin;
+            launch_sat(frames + f0 * fstride, fstride, pitch, nf, h->height, h->width, sat, sat2, s);
+            dinv_kernel<<<dim3(unsigned((h->width - h->W + 1 + 127) / 128), unsigned(h->height - h->W + 1), unsigned(nf)),
+                          128, 0, s>>>(sat, sat2, h->sat_size(), h->height, h->width, h->W, dinv, h->pixels());
+            CorrArgs a{};
+            a.frames = frames + f0 * fstride;
+            a.fstride = fstride;
+            a.pitch = pitch;
+            a.sat = sat;
+            a.sat_fstride = h->sat_size();
+            a.dinv = dinv;
+            a.dinv_fstride = h->pixels();
+            a.h = h->height;
+            a.w = h->width;
+            a.W = h->W;
+            a.R = h->R;
+            a.L = h->L;
+            a.M = h->M;
+            a.nx = h->nx;
+            a.nwin = nwin;
+            a.nf = nf;
+            a.stat = h->stat;
+            a.down = h->d_down.p;
+            a.across = h->d_across.p;
+            a.norm = h->d_norm.p;
+            a.spec = h->d_spec.p;
+            a.twiddles = h->d_tw.p;
+            a.gross = gross_mode == B200_GROSS_FRAME ? gross + 2 * size_t(f0)
+                    : gross_mode == B200_GROSS_WINDOW ? gross + 2 * q0 : nullptr;
+            a.gross_mode = gross_mode;
+            a.offset = offset + 2 * q0;
+            a.peak = peak + q0;
+            a.snr = snr + q0;
+            a.cov = cov + 3 * q0;
+            a.surface = nullptr;
+            B200_DISPATCH(h->N, launch_corr, a, s);
+            CK(cudaGetLastError());
+            h->launches += 4;
+        }
+    });
 }
 
 int b200_sat_device(const uint8_t *frames, int n, int height, int width, int pitch, uint32_t *sat, int64_t *sat2,
