@@ -129,6 +129,13 @@ B200_API int b200_correlate_device_noalloc(b200_handle *h, const uint8_t *frames
 B200_API int b200_sat_device(const uint8_t *frames, int n, int height, int width, int pitch, uint32_t *sat,
                     int64_t *sat2, void *stream);
 
+/* A check of the tensor-core path: D (128 x N, float32) = A (128 x K) x B^T (B is N x K), both
+ * float16 row-major device arrays, computed by one CTA with tcgen05.mma from operands staged in
+ * shared memory K-major or MN-major (a_mn, b_mn), B negated if neg_b; N, K multiples of 16 up to
+ * 256. Synchronous. B200_ETIMEOUT if the MMA completion wait gave up. No reference counterpart. */
+B200_API int b200_tc_selftest(const void *A, const void *B, float *D, int N, int K, int a_mn, int b_mn,
+                              int neg_b, void *stream);
+
 /* The arithmetic of the transforms, B200_FORM_*; B200_EINVAL for an unknown or unbuilt form. */
 B200_API int b200_set_form(b200_handle *h, int form);
 

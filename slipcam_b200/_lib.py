@@ -36,6 +36,7 @@ SIGNATURES = {
     'b200_correlate_device_noalloc': (_i, [_vp, _u8p, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp]),
     'b200_sat_device': (_i, [_u8p, _i, _i, _i, _i, _vp, _vp, _vp]),
     'b200_set_form': (_i, [_vp, _i]),
+    'b200_tc_selftest': (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _vp]),
     'b200_info': (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i),
                        ctypes.POINTER(ctypes.c_uint64)]),
     'b200_profile': (_i, [_vp, _i]),

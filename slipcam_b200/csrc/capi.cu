@@ -20,6 +20,7 @@
 #include "../../include/slipcam_b200.h"
 #include "corr_fft.cuh"
 #include "sat.cuh"
+#include "tc_selftest.cuh"
 
 using namespace b200;
 
@@ -671,6 +672,26 @@ int b200_correlate_device_noalloc(b200_handle *h, const uint8_t *frames, int n, 
             h->launches += 4;
         }
     });
+}
+
+int b200_tc_selftest(const void *A, const void *B, float *D, int N, int K, int a_mn, int b_mn, int neg_b, void *stream)
+{
+    if (!A || !B || !D || N < 16 || N > 256 || N % 16 || K < 16 || K % 16 || K > 256) return B200_EINVAL;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int *status = nullptr;
+    if (cudaMallocAsync(&status, sizeof(int), s) != cudaSuccess) return B200_ERUNTIME;
+    cudaMemsetAsync(status, 0, sizeof(int), s);
+    TcSelftestArgs a{static_cast<const __half *>(A), static_cast<const __half *>(B), D, N, K, a_mn, b_mn, neg_b, status};
+    const size_t smem = size_t(128 + N) * K * 2;
+    if (cudaFuncSetAttribute(tc_selftest_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+        return B200_ERUNTIME;
+    tc_selftest_kernel<<<1, 128, smem, s>>>(a);
+    int h = 0;
+    const bool ok = cudaGetLastError() == cudaSuccess && cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, s) == cudaSuccess
+                    && cudaStreamSynchronize(s) == cudaSuccess;
+    cudaFreeAsync(status, s);
+    if (!ok) return B200_ERUNTIME;
+    return h ? B200_ETIMEOUT : B200_OK;
 }
 
 int b200_sat_device(const uint8_t *frames, int n, int height, int width, int pitch, uint32_t *sat, int64_t *sat2,
