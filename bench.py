@@ -191,6 +191,7 @@ def run_b200(args):
     frames, motion, step, gross = synth.hd(n=NFRAMES, device='cuda', count=args.video)
     gross_d = torch.as_tensor(gross).cuda()
     cor = framecor.Correlator(H, W_, down, across, window=WIN, search=SEARCH, backend='b200', device=local)
+    cor.set_form(args.form)
     cor.set_reference(frames[0])
     fft_n = cor.info()[2]
     BATCH = args.batch
@@ -323,6 +324,7 @@ def main():
     p.add_argument('--no-e2e', action='store_true', help='device timing only (profiling runs)')
     p.add_argument('--video', type=int, default=NFRAMES, help='frames of the synthetic video to render')
     p.add_argument('--batch', type=int, default=BATCH, help='frames per step')
+    p.add_argument('--form', default='fft32', choices=['fft32', 'tc'], help='the arithmetic of the transforms')
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == 'reference':

@@ -52,6 +52,7 @@ extern "C" {
 /* the arithmetic of the transforms */
 #define B200_FORM_AUTO 0   /* the library's choice */
 #define B200_FORM_FFT32 1  /* FP32 FFTs on the CUDA cores */
+#define B200_FORM_TC 2     /* DFT-matrix GEMMs on the tensor cores, FP16 operands, FP32 accumulation */
 
 /* The frames, the grid of reference windows and the correlation parameters.
  * Replaces framecor::Params (cxx/framecor.h:22-35); same fields, same defaults in the binding

@@ -11,7 +11,7 @@ LIB_PATH = os.path.join(HERE, 'libslipcam_b200.so')
 
 OK, EINVAL, ERUNTIME, ETIMEOUT = 0, 1, 2, 3
 GROSS_NONE, GROSS_FRAME, GROSS_WINDOW = 0, 1, 2
-FORM_AUTO, FORM_FFT32 = 0, 1
+FORM_AUTO, FORM_FFT32, FORM_TC = 0, 1, 2
 
 
 class Params(ctypes.Structure):

@@ -17,8 +17,11 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "../../include/slipcam_b200.h"
 #include "corr_fft.cuh"
+#include "corr_tc.cuh"
 #include "sat.cuh"
 #include "tc_selftest.cuh"
 
@@ -123,6 +126,101 @@ void launch_corr(const CorrArgs &a, cudaStream_t s)
     corr_kernel<N, kThreads><<<unsigned(a.nwin) * a.nf, kThreads, Geo<N>::smem_bytes, s>>>(a);
 }
 
+int g_num_sms[64] = {};
+
+int num_sms()
+{
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return 148;
+    if (!g_num_sms[dev]) CK(cudaDeviceGetAttribute(&g_num_sms[dev], cudaDevAttrMultiProcessorCount, dev));
+    return g_num_sms[dev];
+}
+
+// cuTensorMapEncodeTiled, from the driver through the runtime (no link against libcuda)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !p) fail(B200_ERUNTIME, "cuTensorMapEncodeTiled is not available");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// the variance denominators of a group (nf frames of h x w floats) as a 3-D TMA tensor, box
+// tc_box_width(M) x M x 1
+CUtensorMap dinv_map(const float *dinv, int h, int w, int dpitch, int nf, int M)
+{
+    CUtensorMap m{};
+    const cuuint64_t dims[3] = {cuuint64_t(w), cuuint64_t(h), cuuint64_t(nf)};
+    const cuuint64_t strides[2] = {cuuint64_t(dpitch) * 4, cuuint64_t(dpitch) * h * 4};
+    const cuuint32_t box[3] = {cuuint32_t(tc_box_width(M)), cuuint32_t(M), 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(dinv), dims, strides,
+                                            box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) fail(B200_ERUNTIME, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
+    return m;
+}
+
+template <int N>
+void launch_corr_tc(const CorrArgs &a, const uint4 *dtab, int *status, const CUtensorMap *dmap, cudaStream_t s)
+{
+    static bool done[64] = {};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        CK(cudaFuncSetAttribute(corr_tc_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TcGeo<N>::smem_bytes)));
+        done[dev] = true;
+    }
+    const int pairs = a.nwin * a.nf;
+    const int grid = std::min(pairs, num_sms());
+    corr_tc_kernel<N><<<unsigned(grid), kTcThreads, TcGeo<N>::smem_bytes, s>>>(a, dtab, status, dmap);
+}
+
+template <int N>
+bool tc_fits_n(int M)
+{
+    // the surface (A region, M x M floats) and the box of variance denominators (X region)
+    return size_t(M) * M * 4 <= TcGeo<N>::A_BYTES && size_t(tc_box_width(M)) * M * 4 <= TcGeo<N>::X_BYTES;
+}
+
+// whether the tensor-core kernel holds this geometry: FFT size up to 160, up to 128 shifts per axis
+bool tc_fits(int N, int M)
+{
+    if (M > 128) return false;
+    switch (N) {
+    case 16: return tc_fits_n<16>(M);
+    case 32: return tc_fits_n<32>(M);
+    case 48: return tc_fits_n<48>(M);
+    case 64: return tc_fits_n<64>(M);
+    case 80: return tc_fits_n<80>(M);
+    case 96: return tc_fits_n<96>(M);
+    case 128: return tc_fits_n<128>(M);
+    case 144: return tc_fits_n<144>(M);
+    case 160: return tc_fits_n<160>(M);
+    default: return false;
+    }
+}
+
+#define B200_DISPATCH_TC(N_, F, ...)                                                               \
+    switch (N_) {                                                                                   \
+    case 16: F<16>(__VA_ARGS__); break;                                                             \
+    case 32: F<32>(__VA_ARGS__); break;                                                             \
+    case 48: F<48>(__VA_ARGS__); break;                                                             \
+    case 64: F<64>(__VA_ARGS__); break;                                                             \
+    case 80: F<80>(__VA_ARGS__); break;                                                             \
+    case 96: F<96>(__VA_ARGS__); break;                                                             \
+    case 128: F<128>(__VA_ARGS__); break;                                                           \
+    case 144: F<144>(__VA_ARGS__); break;                                                           \
+    case 160: F<160>(__VA_ARGS__); break;                                                           \
+    default: fail(B200_EINVAL, "no tensor-core kernel for the FFT size " + std::to_string(N_));    \
+    }
+
 template <int N>
 void launch_spectra(const SpectraArgs &a, int nwin, cudaStream_t s)
 {
@@ -174,6 +272,10 @@ struct b200_handle {
     DevBuf<int64_t> d_sat2;
     DevBuf<float> d_dinv;
     Slot slot[2];
+    DevBuf<uint16_t> d_dtab;     // the FP16 DFT matrices of the tensor-core form
+    DevBuf<int> d_status;        // device status word (3: a tensor-core wait gave up)
+    DevBuf<CUtensorMap> d_tmaps; // TMA maps of the three denominator tables: slot 0, slot 1, device path
+    bool tc_ok = false;          // the geometry fits the tensor-core kernel
     int fpitch = 0;              // the pitch of the staged frames (a multiple of 16)
     bool profiling = false;      // events around the correlation launches
     struct Timed {
@@ -194,6 +296,8 @@ struct b200_handle {
 
     int64_t sat_size() const { return int64_t(height + 1) * (width + 1); }
     int64_t pixels() const { return int64_t(height) * width; }
+    int dpitch() const { return (width + 3) & ~3; }                  // rows of 16-byte multiples
+    int64_t dinv_size() const { return int64_t(height) * dpitch(); }
 
     // the tables and the correlation of nf frames (device memory) on stream s
     void run_group(const uint8_t *frames, int pitch, int nf, const int32_t *gross, int gross_mode,
@@ -203,7 +307,7 @@ struct b200_handle {
         const int64_t fstride = int64_t(pitch) * height;
         launch_sat(frames, fstride, pitch, nf, height, width, sat, sat2, s);
         dinv_kernel<<<dim3(unsigned((width - W + 1 + 127) / 128), unsigned(height - W + 1), unsigned(nf)), 128, 0, s>>>(
-            sat, sat2, sat_size(), height, width, W, dinv, pixels());
+            sat, sat2, sat_size(), height, width, W, dinv, dinv_size(), dpitch());
         CorrArgs a{};
         a.frames = frames;
         a.fstride = fstride;
@@ -211,7 +315,8 @@ struct b200_handle {
         a.sat = sat;
         a.sat_fstride = sat_size();
         a.dinv = dinv;
-        a.dinv_fstride = pixels();
+        a.dinv_fstride = dinv_size();
+        a.dpitch = dpitch();
         a.h = height;
         a.w = width;
         a.W = W;
@@ -241,7 +346,15 @@ struct b200_handle {
             t.pairs = uint64_t(nf) * nwin;
             CK(cudaEventRecord(t.a, s));
         }
-        B200_DISPATCH(N, launch_corr, a, s);
+        if (form == B200_FORM_TC) {
+            const uint4 *dt = reinterpret_cast<const uint4 *>(d_dtab.p);
+            const int mi = dinv == slot[0].dinv.p ? 0 : dinv == slot[1].dinv.p ? 1 : 2;
+            if (mi == 2 && dinv != d_dinv.p) fail(B200_EINVAL, "no TMA map for this denominator table");
+            const CUtensorMap *dm = d_tmaps.p + mi;
+            B200_DISPATCH_TC(N, launch_corr_tc, a, dt, d_status.p, dm, s);
+        } else {
+            B200_DISPATCH(N, launch_corr, a, s);
+        }
         CK(cudaGetLastError());
         if (profiling) {
             CK(cudaEventRecord(t.b, s));
@@ -326,6 +439,20 @@ void upload_reference(b200_handle *h, const uint8_t *dframe, int pitch, cudaStre
 
 }   // namespace
 
+void b200::tc_dft_table(int N, uint16_t *out)
+{
+    const uint32_t sbo = uint32_t(N / 8) * 128u, bytes = uint32_t(N / 8) * sbo;
+    for (int part = 0; part < 2; ++part)
+        for (int r = 0; r < N; ++r)
+            for (int c = 0; c < N; ++c) {
+                double cc = 0.0, sn = 0.0;
+                cs2pi(long(r) * c, N, cc, sn);
+                const __half hv = __float2half_rn(float(part == 0 ? cc : -sn));
+                const uint32_t off = part * bytes + tc::k_major_offset(r, c, sbo, 128);
+                out[off / 2] = __half_as_ushort(hv);
+            }
+}
+
 extern "C" {
 
 int b200_create(const b200_params *p, int device, b200_handle **out)
@@ -375,15 +502,24 @@ int b200_create(const b200_params *p, int device, b200_handle **out)
         h->d_tw.alloc(tw.size());
         CK(cudaMemcpy(h->d_tw.p, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice));
         h->d_ref.alloc(size_t(h->height) * h->fpitch);
+        h->d_status.alloc(1);
+        CK(cudaMemset(h->d_status.p, 0, sizeof(int)));
+        h->tc_ok = tc_fits(N, h->M);
+        if (h->tc_ok) {
+            std::vector<uint16_t> dt(2 * size_t(N) * N);
+            tc_dft_table(N, dt.data());
+            h->d_dtab.alloc(dt.size());
+            CK(cudaMemcpy(h->d_dtab.p, dt.data(), dt.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+        }
         const size_t G = size_t(h->group), P = G * h->nwin;
         h->d_sat.alloc(G * h->sat_size());
         h->d_sat2.alloc(G * h->sat_size());
-        h->d_dinv.alloc(G * h->pixels());
+        h->d_dinv.alloc(G * h->dinv_size());
         for (Slot &s : h->slot) {
             s.frames.alloc(G * h->height * h->fpitch);
             s.sat.alloc(G * h->sat_size());
             s.sat2.alloc(G * h->sat_size());
-            s.dinv.alloc(G * h->pixels());
+            s.dinv.alloc(G * h->dinv_size());
             s.gross.alloc(2 * P);
             s.out.alloc(7 * P);
             s.hframes.alloc(G * h->height * h->fpitch);
@@ -391,6 +527,13 @@ int b200_create(const b200_params *p, int device, b200_handle **out)
             s.hout.alloc(7 * P);
             CK(cudaEventCreateWithFlags(&s.in, cudaEventDisableTiming));
             CK(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+        }
+        if (h->tc_ok) {
+            const CUtensorMap maps[3] = {dinv_map(h->slot[0].dinv.p, h->height, h->width, h->dpitch(), int(G), h->M),
+                                         dinv_map(h->slot[1].dinv.p, h->height, h->width, h->dpitch(), int(G), h->M),
+                                         dinv_map(h->d_dinv.p, h->height, h->width, h->dpitch(), int(G), h->M)};
+            h->d_tmaps.alloc(3);
+            CK(cudaMemcpy(h->d_tmaps.p, maps, sizeof(maps), cudaMemcpyHostToDevice));
         }
         *out = h;
         g_create_error.clear();
@@ -421,8 +564,12 @@ const char *b200_last_error(const b200_handle *h) { return h ? h->err.c_str() : 
 int b200_set_form(b200_handle *h, int form)
 {
     return guarded(h, [&] {
-        if (form != B200_FORM_AUTO && form != B200_FORM_FFT32) fail(B200_EINVAL, "unknown form " + std::to_string(form));
-        h->form = B200_FORM_FFT32;
+        if (form != B200_FORM_AUTO && form != B200_FORM_FFT32 && form != B200_FORM_TC)
+            fail(B200_EINVAL, "unknown form " + std::to_string(form));
+        if (form == B200_FORM_TC && !h->tc_ok)
+            fail(B200_EINVAL, "the tensor-core form holds FFT sizes up to 160 and search ranges up to 63 px, not "
+                                  + std::to_string(h->N) + " and " + std::to_string(h->R));
+        h->form = form == B200_FORM_AUTO ? B200_FORM_FFT32 : form;
     });
 }
 
@@ -510,6 +657,12 @@ int b200_correlate(b200_handle *h, const uint8_t *frames, int n, const int32_t *
             CK(cudaEventRecord(s.done, h->comp));
         }
         for (int g = std::max(0, ngroups - 2); g < ngroups; ++g) drain(g);
+        int st = 0;
+        CK(cudaMemcpy(&st, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (st) {
+            CK(cudaMemset(h->d_status.p, 0, sizeof(int)));
+            fail(B200_ETIMEOUT, "a tensor-core completion wait gave up; the outputs are not valid");
+        }
     });
 }
 
@@ -604,7 +757,7 @@ int b200_correlate_device_noalloc(b200_handle *h, const uint8_t *frames, int n, 
             fail(B200_EINVAL, "null input or output, or a pitch below the width");
         // the tables of one frame: 32-bit and 64-bit summed-area tables, variance denominators
         const size_t b32 = size_t(h->sat_size()) * sizeof(uint32_t), b64 = size_t(h->sat_size()) * sizeof(int64_t);
-        const size_t bd = size_t(h->pixels()) * sizeof(float);
+        const size_t bd = size_t(h->dinv_size()) * sizeof(float);
         const size_t per_frame = align256(b32) + align256(b64) + align256(bd);
         if (per_frame > kNoAllocBytes)
             fail(B200_EINVAL, "the frame is too large for the no-allocation entry point: its tables need "
@@ -635,7 +788,7 @@ int b200_correlate_device_noalloc(b200_handle *h, const uint8_t *frames, int n, 
             const size_t q0 = size_t(f0) * nwin;
             launch_sat(frames + f0 * fstride, fstride, pitch, nf, h->height, h->width, sat, sat2, s);
             dinv_kernel<<<dim3(unsigned((h->width - h->W + 1 + 127) / 128), unsigned(h->height - h->W + 1), unsigned(nf)),
-                          128, 0, s>>>(sat, sat2, h->sat_size(), h->height, h->width, h->W, dinv, h->pixels());
+                          128, 0, s>>>(sat, sat2, h->sat_size(), h->height, h->width, h->W, dinv, h->dinv_size(), h->dpitch());
             CorrArgs a{};
             a.frames = frames + f0 * fstride;
             a.fstride = fstride;
@@ -643,7 +796,8 @@ int b200_correlate_device_noalloc(b200_handle *h, const uint8_t *frames, int n, 
             a.sat = sat;
             a.sat_fstride = h->sat_size();
             a.dinv = dinv;
-            a.dinv_fstride = h->pixels();
+            a.dinv_fstride = h->dinv_size();
+            a.dpitch = h->dpitch();
             a.h = h->height;
             a.w = h->width;
             a.W = h->W;

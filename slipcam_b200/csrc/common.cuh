@@ -49,8 +49,9 @@ struct CorrArgs {
     int pitch;
     const uint32_t *sat;       // nf x (h + 1) x (w + 1): the summed-area table of the pixels
     int64_t sat_fstride;       // elements per frame
-    const float *dinv;         // nf x h x w: 1 / sqrt(variance * n) of each W x W box (0 if flat)
+    const float *dinv;         // nf x h x dpitch: 1 / sqrt(variance * n) of each W x W box (0 if flat)
     int64_t dinv_fstride;
+    int dpitch;                // floats per row of dinv: the width rounded up to 4 (16-byte rows)
     int h, w, W, R, L, M, nx, nwin, nf, stat;
     const int *down, *across;
     const float *norm;         // nwin

@@ -41,18 +41,20 @@ B200_HD void peak_outputs(const float *s, int pitch, int M, int u, int v, int R,
         double f[3][3];
         for (int i = 0; i < 3; i++)
             for (int j = 0; j < 3; j++) f[i][j] = s[(u + i - 1) * pitch + v + j - 1];
-        const double c1 = (f[2][0] + f[2][1] + f[2][2] - f[0][0] - f[0][1] - f[0][2]) / 6;
-        const double c2 = (f[0][2] + f[1][2] + f[2][2] - f[0][0] - f[1][0] - f[2][0]) / 6;
+        constexpr double sixth = 1.0 / 6.0;   // the surface.h divisions by 6 and 4, as products
+        const double c1 = (f[2][0] + f[2][1] + f[2][2] - f[0][0] - f[0][1] - f[0][2]) * sixth;
+        const double c2 = (f[0][2] + f[1][2] + f[2][2] - f[0][0] - f[1][0] - f[2][0]) * sixth;
         const double c3 = (f[0][0] + f[0][1] + f[0][2] + f[2][0] + f[2][1] + f[2][2]
-                           - 2 * (f[1][0] + f[1][1] + f[1][2])) / 6;
+                           - 2 * (f[1][0] + f[1][1] + f[1][2])) * sixth;
         const double c5 = (f[0][0] + f[1][0] + f[2][0] + f[0][2] + f[1][2] + f[2][2]
-                           - 2 * (f[0][1] + f[1][1] + f[2][1])) / 6;
-        const double c4 = (f[2][2] - f[2][0] - f[0][2] + f[0][0]) / 4;
+                           - 2 * (f[0][1] + f[1][1] + f[2][1])) * sixth;
+        const double c4 = (f[2][2] - f[2][0] - f[0][2] + f[0][0]) * 0.25;
         const double det = 4 * c3 * c5 - c4 * c4;
         bool fitted = false;
         if (c3 < 0 && det > 0) {
-            du = (c4 * c2 - 2 * c5 * c1) / det;
-            dv = (c4 * c1 - 2 * c3 * c2) / det;
+            const double rdet = 1.0 / det;
+            du = (c4 * c2 - 2 * c5 * c1) * rdet;
+            dv = (c4 * c1 - 2 * c3 * c2) * rdet;
             fitted = fabs(du) <= 1 && fabs(dv) <= 1;
         }
         if (!fitted) {
@@ -78,10 +80,10 @@ B200_HD void peak_outputs(const float *s, int pitch, int M, int u, int v, int R,
         n2 *= 2;
         const double w = dxy * dxy - dxx * dyy;
         if (fabs(w) >= 1e-2) {
-            const double w2 = w * w;
-            cov[3 * q] = float((-n2 * w * dyy + n4 * (dyy * dyy + dxy * dxy)) / w2);
-            cov[3 * q + 1] = float((-n2 * w * dxx + n4 * (dxx * dxx + dxy * dxy)) / w2);
-            cov[3 * q + 2] = float((n2 * w * dxy - n4 * (dxx + dyy) * dxy) / w2);
+            const double rw2 = 1.0 / (w * w);
+            cov[3 * q] = float((-n2 * w * dyy + n4 * (dyy * dyy + dxy * dxy)) * rw2);
+            cov[3 * q + 1] = float((-n2 * w * dxx + n4 * (dxx * dxx + dxy * dxy)) * rw2);
+            cov[3 * q + 2] = float((n2 * w * dxy - n4 * (dxx + dyy) * dxy) * rw2);
         }
     }
 }
@@ -244,8 +246,8 @@ __global__ void __launch_bounds__(NT, (N <= 160 ? 2 : 1)) corr_kernel(CorrArgs a
     // back to rows, normalized: rho = c / (N^2) / (norm sqrt(n var)), the variance term from the
     // precomputed table of the frame (0 where the search box is flat)
     const float inv = 1.0f / (float(N) * float(N) * norm);
-    const float *dinv = a.dinv + size_t(f) * a.dinv_fstride + size_t(sy) * a.w + sx;
-    const int dw = a.w;
+    const float *dinv = a.dinv + size_t(f) * a.dinv_fstride + size_t(sy) * a.dpitch + sx;
+    const int dw = a.dpitch;
     row_inverse<N>(ex, S, M, TWI, [&](int u, int c, float x) { return x * inv * __ldg(dinv + size_t(u) * dw + c); });
     __syncthreads();
     if (a.surface)

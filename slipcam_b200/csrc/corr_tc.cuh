@@ -1,0 +1,523 @@
+// corr_tc.cuh -- the tensor-core form: the 2-D DFTs of the correlation as dense DFT-matrix GEMMs
+// on tcgen05 (FP16 operands, FP32 accumulation in TMEM), one (window, frame) pair at a time per
+// persistent CTA. With D = [w_N^{rc}] (Dr = cos, Di = -sin, N x N, resident in shared memory as
+// FP16) every stage is a GEMM whose fixed operand is a block of Dr or Di:
+//
+//   S1  Y  = X Dr|Di          rows i (chip rows), K = j, N = kappa (Re | Im)     X = chip - round(mean)
+//   S2  Z^T = Y^T D            rows kappa, K = (Re|Im, i), N = (Re|Im, ky)        A2 MN-major from S1's rows
+//   S3  P = Z conj(R) 2^-s     per thread (one kappa row), R the resident reference spectrum
+//   S4  Q^T = P^T conj(D)      rows kappa, K = (Re|Im, ky), N = (Re|Im, u < M)    A4 K-major from S3's rows
+//   S5  c^T = [Dr|Di] (w Q)    rows v, K = (Re|Im, kappa), N = u                  B5 MN-major from S4's rows
+//
+// then the normalization by the variance denominators, the argmax and the FP64 peak epilogue of
+// the FP32 form. Each stage writes the next stage's operand straight from its TMEM rows: a thread
+// owns one accumulator row and stores it as 16-byte chunks, in the major order the next GEMM reads.
+// Power-of-two scales keep every FP16 operand in range: |X| <= 255, |Y| <= 255 N, the reference
+// spectrum is scaled by 2^-e with 2^e > W * norm >= max |R|, P by 2^-8 (|P| <= N^2 255 2^-8 < 2^15
+// for N <= 160) and w Q by 2^-9. Fixed-size tensor-core tiles: rows beyond the data (chip rows >= N, kappa rows
+// >= KP, output rows >= M) read whatever follows in shared memory and their results are ignored.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_fp16.h>
+
+#include "corr_fft.cuh"
+#include "tc.cuh"
+
+namespace b200 {
+
+constexpr uint32_t cmax(uint32_t a, uint32_t b) { return a > b ? a : b; }
+
+template <int N>
+struct TcGeo {
+    static constexpr int NH = N / 2 + 1;                            // frequencies of a real row
+    static constexpr int KP = (NH + 15) / 16 * 16;                  // kappa rows, padded
+    static constexpr int T1 = (N + 127) / 128;                      // row tiles of S1
+    static constexpr uint32_t SBO_D = uint32_t(N / 8) * 128u;       // Dr, Di, X: K-major rows of N
+    static constexpr uint32_t SBO_A = uint32_t(2 * N / 8) * 128u;   // A2 (MN-major), A4 (K-major): K = 2N
+    static constexpr uint32_t SBO_B5 = uint32_t(2 * KP / 8) * 128u; // B5 (MN-major): K = 2 KP
+    static constexpr uint32_t A_BYTES = uint32_t(KP / 8) * SBO_A;
+    static constexpr uint32_t X_BYTES = cmax(uint32_t(N / 8) * SBO_D, 16u * SBO_B5);
+    static constexpr uint32_t D_BYTES = uint32_t(N / 8) * SBO_D;
+    static constexpr uint32_t OFF_X = A_BYTES, OFF_DR = OFF_X + X_BYTES, OFF_DI = OFF_DR + D_BYTES;
+    static constexpr uint32_t END = OFF_DI + D_BYTES;
+    // the furthest byte a full 128-row tile reads
+    static constexpr uint32_t READ_END = cmax(cmax(16u * SBO_A, OFF_X + uint32_t(T1) * 16u * SBO_D),
+                                              cmax(OFF_DI + 16u * SBO_D, END));
+    static constexpr size_t smem_bytes = READ_END;
+    static constexpr uint32_t TMEM_COLS = 512;
+    static_assert(KP <= 128 && T1 * 2 * KP <= 512 && 2 * N <= 512, "TMEM or tile bounds");
+    static_assert(READ_END <= 227 * 1024, "shared memory");
+};
+
+#ifdef __CUDACC__
+
+__device__ __forceinline__ uint4 pack8(const float *v, float s)
+{
+    uint4 r;
+    __half2 h0 = __floats2half2_rn(v[0] * s, v[1] * s), h1 = __floats2half2_rn(v[2] * s, v[3] * s);
+    __half2 h2 = __floats2half2_rn(v[4] * s, v[5] * s), h3 = __floats2half2_rn(v[6] * s, v[7] * s);
+    r.x = *reinterpret_cast<uint32_t *>(&h0);
+    r.y = *reinterpret_cast<uint32_t *>(&h1);
+    r.z = *reinterpret_cast<uint32_t *>(&h2);
+    r.w = *reinterpret_cast<uint32_t *>(&h3);
+    return r;
+}
+
+__device__ __forceinline__ uint4 pack8(const float *v)
+{
+    uint4 r;
+    __half2 h0 = __floats2half2_rn(v[0], v[1]), h1 = __floats2half2_rn(v[2], v[3]);
+    __half2 h2 = __floats2half2_rn(v[4], v[5]), h3 = __floats2half2_rn(v[6], v[7]);
+    r.x = *reinterpret_cast<uint32_t *>(&h0);
+    r.y = *reinterpret_cast<uint32_t *>(&h1);
+    r.z = *reinterpret_cast<uint32_t *>(&h2);
+    r.w = *reinterpret_cast<uint32_t *>(&h3);
+    return r;
+}
+
+// the MMAs of the current phase have completed: one thread polls the mbarrier, the others wait at
+// the barrier; false (for all threads) if the poll gave up
+__device__ __forceinline__ bool tc_wait_all(uint64_t *mbar, uint32_t &phase)
+{
+    bool ok = true;
+    if (threadIdx.x == 0) ok = tc::mbar_wait(mbar, phase);
+    phase ^= 1u;
+    const bool failed = __syncthreads_or(!ok);
+    tc::fence_after_sync();
+    return !failed;
+}
+
+// 4 pixels (a little-endian word) minus the same offset, as two exact FP16 pairs: a byte b placed
+// under the exponent byte 0x64 reads as the half 1024 + b, and 1024 + b - (1024 + m) is exact
+__device__ __forceinline__ void bytes_to_half(uint32_t word, __half2 off, uint32_t &lo, uint32_t &hi)
+{
+    uint32_t a = __byte_perm(word, 0x64646464u, 0x4140);   // (1024 + b0, 1024 + b1)
+    uint32_t b = __byte_perm(word, 0x64646464u, 0x4342);   // (1024 + b2, 1024 + b3)
+    __half2 ha = __hsub2(*reinterpret_cast<__half2 *>(&a), off);
+    __half2 hb = __hsub2(*reinterpret_cast<__half2 *>(&b), off);
+    lo = *reinterpret_cast<uint32_t *>(&ha);
+    hi = *reinterpret_cast<uint32_t *>(&hb);
+}
+
+// shared-memory operands written by this thread become visible to the tensor core
+__device__ __forceinline__ void tc_publish()
+{
+    tc::fence_smem_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+}
+
+// two warps per TMEM lane quadrant: warp w and w + 4 own the same 32 accumulator rows and split
+// their columns
+constexpr int kTcThreads = 256;
+
+// the rows of the variance-denominator box a TMA copy brings in: x rounded down to 4 floats
+// (16 bytes), so BW = M + 3 rounded up to 4 floats per row
+__host__ __device__ constexpr int tc_box_width(int M) { return (M + 3 + 3) / 4 * 4; }
+
+// dmap (global memory): the variance denominators of the group as a 3-D tensor (x = column,
+// y = row, z = frame), box tc_box_width(M) x M x 1
+template <int N>
+__global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, const uint4 *dtab, int *status,
+                                                                  const CUtensorMap *dmap)
+{
+    using G = TcGeo<N>;
+    constexpr int NH = G::NH, KP = G::KP, NT = kTcThreads;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ uint32_t tmem_base;
+    __shared__ __align__(8) uint64_t mbar, tbar;
+    __shared__ float s_best[NT / 32];
+    __shared__ int s_at[NT / 32];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int quad = warp & 3, half = warp >> 2;
+    const int row = 32 * quad + lane;   // this thread's accumulator row (TMEM lane)
+    unsigned char *A = smem, *X = smem + G::OFF_X;
+    float *surf = reinterpret_cast<float *>(A);        // the surface, after S5 (A region)
+    float *dvs = reinterpret_cast<float *>(X);         // the variance denominators, from S2 on (X region)
+    const uint32_t sA = tc::smem_u32(A), sX = tc::smem_u32(X);
+    const uint32_t sDR = tc::smem_u32(smem + G::OFF_DR), sDI = tc::smem_u32(smem + G::OFF_DI);
+
+    // the DFT matrices (already in the K-major layout), once per CTA
+    for (int i = tid; i < int(2 * G::D_BYTES / 16); i += NT)
+        reinterpret_cast<uint4 *>(smem + G::OFF_DR)[i] = __ldg(dtab + i);
+    if (warp == 0) tc::tmem_alloc(&tmem_base, G::TMEM_COLS);
+    if (tid == 0) {
+        tc::mbar_init(&mbar, 1);
+        tc::mbar_init(&tbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_publish();
+    const uint32_t tmem = tmem_base;
+    uint32_t tphase = 0;
+    const int BW = tc_box_width(a.M);
+    const uint32_t lane_base = uint32_t(32 * quad) << 16;
+    // the descriptors at k = 0 (built where they are used); the k-step s starts 256 s bytes on
+    // (16 s in the start-address field)
+#define B200_TC_DESCS                                                                                  \
+    const uint64_t dR0 = tc::smem_desc(sDR, 128, G::SBO_D), dI0 = tc::smem_desc(sDI, 128, G::SBO_D); \
+    const uint64_t a0A = tc::smem_desc(sA, 128, G::SBO_A), b0B5 = tc::smem_desc(sA, 128, G::SBO_B5);  \
+    (void)dR0; (void)dI0; (void)a0A; (void)b0B5;
+    uint32_t phase = 0;
+    const int L = a.L, M = a.M, R = a.R, W = a.W;
+    const int NO = (M + 15) / 16 * 16;
+    const int npairs = a.nwin * a.nf;
+    const size_t ss = size_t(a.w) + 1;
+    const bool words = ((a.pitch | reinterpret_cast<uintptr_t>(a.frames) | int(a.fstride)) & 3) == 0;
+
+    // the pair whose peak warp 0 still has to write: the surface stays in the A region until the
+    // next pair's first drain, after the gather
+    struct Pending {
+        int64_t q;
+        int at, gy, gx;
+        bool valid, live;
+    } pend{0, 0, 0, 0, false, false};
+    auto finish_peak = [&](Pending &pp) {
+        if (!pp.live) return;
+        pp.live = false;
+        if (!pp.valid) {
+            if (lane == 0) invalid_outputs(pp.q, a.offset, a.peak, a.snr, a.cov);
+            return;
+        }
+        const int u = pp.at / M, v = pp.at % M;
+        int i0, i1, j0, j1;
+        snr_patch(M, a.stat, u, v, i0, i1, j0, j1);
+        const int pw = j1 - j0, cnt = (i1 - i0) * pw;
+        double sum = 0.0;
+        for (int t = lane; t < cnt; t += 32) {
+            const double c = surf[(i0 + t / pw) * M + j0 + t % pw];
+            sum += c * c;
+        }
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (lane == 0) peak_outputs(surf, M, M, u, v, R, pp.gy, pp.gx, W * W, sum, cnt, pp.q, a.offset, a.peak, a.snr, a.cov);
+    };
+
+    for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
+        if (warp == 0) finish_peak(pend);
+        const int k = p / a.nf, f = p % a.nf;
+        const int64_t q = int64_t(f) * a.nwin + k;
+        int gy = 0, gx = 0;
+        if (a.gross_mode == 1) {
+            gy = a.gross[2 * f];
+            gx = a.gross[2 * f + 1];
+        } else if (a.gross_mode == 2) {
+            gy = a.gross[2 * q];
+            gx = a.gross[2 * q + 1];
+        }
+        const int sy = a.down[k / a.nx] + gy - R, sx = a.across[k % a.nx] + gx - R;
+        const float norm = a.norm[k];
+        if (!(norm > 0) || sy < 0 || sx < 0 || sy + L > a.h || sx + L > a.w) {
+            if (tid == 0) invalid_outputs(q, a.offset, a.peak, a.snr, a.cov);
+            if (a.surface)
+                for (int i = tid; i < M * M; i += NT) a.surface[q * M * M + i] = 0.0f;
+            continue;
+        }
+
+        // ---- X = chip - round(mean), FP16, K-major (rows i, columns j), zero outside L x L. A warp
+        // takes 8 rows x 4 chunks of 8 pixels: 32-byte pieces of 8 rows from global memory, one
+        // contiguous 512-byte store into shared memory. Every load of the thread first.
+        const uint32_t *sat = a.sat + size_t(f) * a.sat_fstride;
+        const uint32_t box = sat[(sy + L) * ss + sx + L] - sat[sy * ss + sx + L] - sat[(sy + L) * ss + sx] + sat[sy * ss + sx];
+        const uint32_t LL = uint32_t(L) * uint32_t(L);
+        const int mean = int((box + LL / 2) / LL);
+        const __half2 off = __float2half2_rn(1024.0f + float(mean));
+        const uint8_t *chip = a.frames + f * a.fstride + int64_t(sy) * a.pitch + sx;
+        {
+            constexpr int NCG = (N / 8 + 3) / 4;               // groups of 4 chunks per row
+            constexpr int NB = (N / 8) * NCG;                   // blocks of 8 rows x 4 chunks
+            constexpr int PERT = (NB + NT / 32 - 1) / (NT / 32);   // blocks per warp
+            constexpr int PERW = (PERT + 1) / 2;                    // in two rounds
+#pragma unroll
+            for (int round = 0; round < 2; ++round) {
+            uint32_t w0[PERW], w1[PERW], w2[PERW];
+#pragma unroll
+            for (int t = 0; t < PERW; ++t) {
+                const int b = warp + (NT / 32) * (t + round * PERW);
+                const int i = 8 * (b / NCG) + (lane & 7), j0 = 8 * (4 * (b % NCG) + (lane >> 3));
+                w0[t] = w1[t] = w2[t] = 0u;
+                if (b < NB && t + round * PERW < PERT && i < L && j0 < L && j0 < N) {
+                    const uint8_t *src = chip + int64_t(i) * a.pitch + j0;
+                    const int left = L - j0;   // chip bytes from src on
+                    if (words) {
+                        // the aligned words holding the chip bytes among src[0 .. 8)
+                        const uintptr_t addr = reinterpret_cast<uintptr_t>(src);
+                        const uint32_t *wp = reinterpret_cast<const uint32_t *>(addr & ~uintptr_t(3));
+                        const int sh = int(addr & 3);
+                        w0[t] = __ldg(wp);
+                        if (4 - sh < left) w1[t] = __ldg(wp + 1);
+                        if (sh > 0 && 8 - sh < left) w2[t] = __ldg(wp + 2);
+                    } else {
+                        for (int e = 0; e < 8 && e < left; ++e) {
+                            const uint32_t bt = __ldg(src + e);
+                            if (e < 4) w0[t] |= bt << (8 * e);
+                            else w1[t] |= bt << (8 * (e - 4));
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < PERW; ++t) {
+                const int b = warp + (NT / 32) * (t + round * PERW);
+                const int i = 8 * (b / NCG) + (lane & 7), j0 = 8 * (4 * (b % NCG) + (lane >> 3));
+                if (b < NB && t + round * PERW < PERT && j0 < N) {
+                    uint4 out = make_uint4(0u, 0u, 0u, 0u);
+                    if (i < L && j0 < L) {
+                        uint32_t lo = w0[t], hi = w1[t];
+                        if (words) {
+                            const int sh = int(reinterpret_cast<uintptr_t>(chip + int64_t(i) * a.pitch + j0) & 3);
+                            lo = __funnelshift_r(w0[t], w1[t], 8 * sh);
+                            hi = __funnelshift_r(w1[t], w2[t], 8 * sh);
+                        }
+                        bytes_to_half(lo, off, out.x, out.y);
+                        bytes_to_half(hi, off, out.z, out.w);
+                        if (j0 + 8 > L) {   // the last chunk of a row: zero past the chip
+                            const int keep = L - j0;   // 1 .. 7 pixels
+                            uint32_t *o = reinterpret_cast<uint32_t *>(&out);
+#pragma unroll
+                            for (int e = 0; e < 4; ++e) {
+                                if (2 * e >= keep) o[e] = 0u;
+                                else if (2 * e + 1 >= keep) o[e] &= 0xFFFFu;
+                            }
+                        }
+                    }
+                    *reinterpret_cast<uint4 *>(X + tc::k_major_offset(i, j0, G::SBO_D, 128)) = out;
+                }
+            }
+            }
+        }
+        tc_publish();
+
+        // ---- S1: Y = X [Dr | Di], tile t of 128 chip rows -> TMEM columns [2 KP t, 2 KP (t + 1))
+        if (tid == 0) {
+            B200_TC_DESCS
+            const uint32_t id = tc::instr_desc(128, KP, false, false, false, false);
+#pragma unroll
+            for (int t = 0; t < G::T1; ++t) {
+                const uint64_t a0 = tc::smem_desc(sX + uint32_t(t * 16) * G::SBO_D, 128, G::SBO_D);
+#pragma unroll 2
+                for (int s = 0; s < N / 16; ++s) {
+                    tc::mma_f16(tmem + uint32_t(2 * KP * t), a0 + 16u * s, dR0 + 16u * s, id, s > 0);
+                    tc::mma_f16(tmem + uint32_t(2 * KP * t + KP), a0 + 16u * s, dI0 + 16u * s, id, s > 0);
+                }
+            }
+            tc::mma_commit(&mbar);
+        }
+        if (!tc_wait_all(&mbar, phase)) {
+            if (tid == 0 && status) atomicExch(status, 3);
+            break;
+        }
+        // S1 -> A2 (MN-major: m = kappa, k = part * N + i); warps w and w + 4 take Re and Im
+        for (int t = 0; t < G::T1; ++t) {
+            if (128 * t + 32 * quad >= N) continue;   // warp-uniform
+            const int i = 128 * t + row;
+#pragma unroll
+            for (int cb = 0; cb < KP; cb += 16 * (KP % 32 ? 1 : 2)) {   // 32 (or 16) columns per wait
+                constexpr int NC = KP % 32 ? 16 : 32;
+                float v[NC];
+                tc::tmem_ld_cols<NC>(tmem + lane_base + uint32_t(2 * KP * t + half * KP + cb), v);
+                if (i < N) {
+#pragma unroll
+                    for (int c0 = 0; c0 < NC; c0 += 8)
+                        *reinterpret_cast<uint4 *>(A + tc::mn_major_offset(cb + c0, half * N + i, G::SBO_A, 128)) = pack8(v + c0);
+                }
+            }
+        }
+        tc_publish();
+
+        // ---- S2: Z^T = Y^T D: Zr in TMEM columns [0, N), Zi in [N, 2N)
+        if (tid == 0) {
+            B200_TC_DESCS
+            const uint32_t id = tc::instr_desc(128, N, true, false, false, false);
+            const uint32_t idn = tc::instr_desc(128, N, true, false, false, true);
+#pragma unroll 2
+            for (int s = 0; s < N / 16; ++s) {
+                const uint64_t ar = a0A + 16u * s, ai = a0A + uint32_t(N + 16 * s);   // Yr: k = i, Yi: k = N + i
+                tc::mma_f16(tmem, ar, dR0 + 16u * s, id, s > 0);        // Zr += Yr Dr
+                tc::mma_f16(tmem, ai, dI0 + 16u * s, idn, 1);           // Zr -= Yi Di
+                tc::mma_f16(tmem + N, ar, dI0 + 16u * s, id, s > 0);    // Zi += Yr Di
+                tc::mma_f16(tmem + N, ai, dR0 + 16u * s, id, 1);        // Zi += Yi Dr
+            }
+            tc::mma_commit(&mbar);
+        }
+        // meanwhile: the variance denominators of this pair into the X region (free after S1)
+        // (one TMA box: rows sy .. sy + M - 1, columns from sx rounded down to 4)
+        if (tid == 0) {
+            tc::mbar_expect_tx(&tbar, uint32_t(BW * M * 4));
+            tc::tma_load_3d(dvs, dmap, sx & ~3, sy, f, &tbar);
+        }
+        // and this thread's row of the reference spectrum (S3)
+        int eR = 0;
+        frexpf(float(W) * norm, &eR);   // W * norm < 2^eR, and max |R| <= W * norm
+        const int kap = row;
+        const float4 *rrow = reinterpret_cast<const float4 *>(a.spec + (size_t(k) * NH + (kap < NH ? kap : 0)) * N);
+        if (!tc_wait_all(&mbar, phase)) {
+            if (tid == 0 && status) atomicExch(status, 3);
+            break;
+        }
+
+        // ---- S3: P = Z conj(R) 2^-(eR + 8) -> A4 (K-major: row kappa, k = part * N + ky); the
+        // 16-column chunks of ky alternate between the two warps of a quadrant
+        if (32 * quad < KP) {
+            const float sc = ldexpf(1.0f, -(eR + 8));
+            float4 rn[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) rn[e] = kap < NH ? __ldg(rrow + 8 * half + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int c0 = 16 * half; c0 < N; c0 += 32) {
+                uint32_t zr[16], zi[16];
+                tc::tmem_ld16_nowait(tmem + lane_base + uint32_t(c0), zr);
+                tc::tmem_ld16_nowait(tmem + lane_base + uint32_t(N + c0), zi);
+                float4 rc[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) rc[e] = rn[e];
+                if (c0 + 32 < N && kap < NH) {
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) rn[e] = __ldg(rrow + (c0 + 32) / 2 + e);
+                }
+                tc::tmem_wait();
+                if (kap < KP) {
+#pragma unroll
+                    for (int hh = 0; hh < 2; ++hh) {   // 8 frequencies at a time
+                        float pr[8], pi[8];
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) {
+                            const float4 r = rc[4 * hh + e];
+                            const int z = 8 * hh + 2 * e;
+                            const float ar = __uint_as_float(zr[z]), ai = __uint_as_float(zi[z]);
+                            const float br = __uint_as_float(zr[z + 1]), bi = __uint_as_float(zi[z + 1]);
+                            pr[2 * e] = (ar * r.x + ai * r.y) * sc;
+                            pi[2 * e] = (ai * r.x - ar * r.y) * sc;
+                            pr[2 * e + 1] = (br * r.z + bi * r.w) * sc;
+                            pi[2 * e + 1] = (bi * r.z - br * r.w) * sc;
+                        }
+                        *reinterpret_cast<uint4 *>(A + tc::k_major_offset(kap, c0 + 8 * hh, G::SBO_A, 128)) = pack8(pr);
+                        *reinterpret_cast<uint4 *>(A + tc::k_major_offset(kap, N + c0 + 8 * hh, G::SBO_A, 128)) = pack8(pi);
+                    }
+                }
+            }
+        }
+        tc_publish();
+
+        // ---- S4: Q^T = P^T conj(D) for u < NO: Qr in TMEM columns [0, NO), Qi in [NO, 2 NO)
+        if (tid == 0) {
+            B200_TC_DESCS
+            const uint32_t id = tc::instr_desc(128, NO, false, false, false, false);
+            const uint32_t idn = tc::instr_desc(128, NO, false, false, false, true);
+#pragma unroll 2
+            for (int s = 0; s < N / 16; ++s) {
+                const uint64_t ar = a0A + 16u * s, ai = a0A + uint32_t(N + 16 * s);   // Pr, Pi
+                tc::mma_f16(tmem, ar, dR0 + 16u * s, id, s > 0);                 // Qr += Pr Dr
+                tc::mma_f16(tmem, ai, dI0 + 16u * s, id, 1);                     // Qr += Pi Di
+                tc::mma_f16(tmem + uint32_t(NO), ar, dI0 + 16u * s, idn, s > 0); // Qi -= Pr Di
+                tc::mma_f16(tmem + uint32_t(NO), ai, dR0 + 16u * s, id, 1);      // Qi += Pi Dr
+            }
+            tc::mma_commit(&mbar);
+        }
+        if (!tc_wait_all(&mbar, phase)) {
+            if (tid == 0 && status) atomicExch(status, 3);
+            break;
+        }
+        // S4 -> B5 in the A region (MN-major: n = u, k = part * KP + kappa), with the Hermitian
+        // weights and 2^-9; warps w and w + 4 take Qr and Qi
+        if (32 * quad < KP) {
+            const int kap = row;
+            const float wgt = kap >= NH ? 0.0f : ((kap == 0 || 2 * kap == N) ? 1.0f : 2.0f) * (1.0f / 512.0f);
+            for (int c0 = 0; c0 < NO; c0 += 32) {
+                uint32_t r[32];
+                tc::tmem_ld16_nowait(tmem + lane_base + uint32_t(half * NO + c0), r);
+                if (c0 + 16 < NO) tc::tmem_ld16_nowait(tmem + lane_base + uint32_t(half * NO + c0 + 16), r + 16);
+                tc::tmem_wait();
+                if (kap < KP) {
+                    float v[32];
+#pragma unroll
+                    for (int e = 0; e < 32; ++e) v[e] = __uint_as_float(r[e]);
+#pragma unroll
+                    for (int h = 0; h < 4; ++h)
+                        if (c0 + 8 * h < NO)
+                            *reinterpret_cast<uint4 *>(A + tc::mn_major_offset(c0 + 8 * h, half * KP + kap, G::SBO_B5, 128)) =
+                                pack8(v + 8 * h, wgt);
+                }
+            }
+        }
+        tc_publish();
+
+        // ---- S5: c^T[v][u] = sum_kappa Dr[v][kappa] B5re[kappa][u] + Di[v][kappa] B5im[kappa][u]
+        if (tid == 0) {
+            B200_TC_DESCS
+            const uint32_t id = tc::instr_desc(128, NO, false, true, false, false);
+#pragma unroll 2
+            for (int s = 0; s < KP / 16; ++s) {
+                tc::mma_f16(tmem, dR0 + 16u * s, b0B5 + 16u * s, id, s > 0);
+                tc::mma_f16(tmem, dI0 + 16u * s, b0B5 + uint32_t(KP + 16 * s), id, 1);
+            }
+            tc::mma_commit(&mbar);
+        }
+        if (tid == 0 && !tc::mbar_wait(&tbar, tphase) && status) atomicExch(status, 3);   // the denominators
+        tphase ^= 1u;
+        if (!tc_wait_all(&mbar, phase)) {
+            if (tid == 0 && status) atomicExch(status, 3);
+            break;
+        }
+
+        // ---- the normalized surface (thread v holds column v), its argmax; 16-column chunks of u
+        // alternate between the two warps of a quadrant
+        const float scale = ldexpf(1.0f, eR + 17) / (float(N) * float(N) * norm);
+        float best = -2.0f;
+        int at = INT_MAX;
+        if (32 * quad < M) {
+            const int v = row;
+            const float *__restrict__ dv = dvs + (sx & 3) + v;
+            float *__restrict__ sv = surf + v;
+            for (int u0 = 16 * half; u0 < NO; u0 += 32) {   // one 16-column chunk of u per TMEM wait
+                uint32_t cr[16];
+                tc::tmem_ld16_nowait(tmem + lane_base + uint32_t(u0), cr);
+                tc::tmem_wait();
+                if (v < M) {
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        const int u = u0 + e;
+                        if (u < M) {
+                            const float rho = __uint_as_float(cr[e]) * scale * dv[u * BW];
+                            sv[u * M] = rho;
+                            if (rho > best) {
+                                best = rho;
+                                at = u;
+                            }
+                        }
+                    }
+                }
+            }
+            at = at == INT_MAX ? INT_MAX : at * M + v;
+        }
+        for (int o = 16; o > 0; o >>= 1) better(best, at, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, at, o));
+        if (lane == 0) {
+            s_best[warp] = best;
+            s_at[warp] = at;
+        }
+        tc::fence_before_sync();
+        __syncthreads();
+        if (a.surface)
+            for (int i = tid; i < M * M; i += NT) a.surface[q * M * M + i] = surf[i];
+        if (warp == 0) {
+            best = lane < NT / 32 ? s_best[lane] : -2.0f;
+            at = lane < NT / 32 ? s_at[lane] : INT_MAX;
+            for (int o = 16; o > 0; o >>= 1) better(best, at, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, at, o));
+            pend = {q, at, gy, gx, best > 0, true};   // finished while the next chip loads
+        }
+        __syncthreads();
+        tc::fence_after_sync();
+    }
+    if (warp == 0) finish_peak(pend);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, G::TMEM_COLS);
+#undef B200_TC_DESCS
+}
+
+#endif   // __CUDACC__
+
+// the DFT matrices of the tensor-core form as the kernel keeps them in shared memory: Dr then Di,
+// each K-major (rows r, columns c, both in [0, N)), FP16 bits; out holds 2 * N * N halves
+void tc_dft_table(int N, uint16_t *out);
+
+}   // namespace b200

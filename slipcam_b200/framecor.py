@@ -100,9 +100,10 @@ class Correlator:
             _lib.raise_for(rc, None)
 
     def __del__(self):
-        if getattr(self, '_h', None):
-            _lib.lib().b200_destroy(self._h)
-            self._h = None
+        h = getattr(self, '_h', None)
+        self._h = None
+        if h and _lib is not None and _lib._lib is not None:
+            _lib._lib.b200_destroy(h)
 
     @property
     def backend(self):
@@ -122,8 +123,9 @@ class Correlator:
         return self._search
 
     def set_form(self, form):
-        """The arithmetic of the transforms: 'fft32' (FP32 FFTs) or 'auto'."""
-        code = {'auto': _lib.FORM_AUTO, 'fft32': _lib.FORM_FFT32}.get(form)
+        """The arithmetic of the transforms: 'fft32' (FP32 FFTs on the CUDA cores), 'tc' (DFT-matrix
+        GEMMs on the tensor cores, FP16 operands, FP32 accumulation) or 'auto'."""
+        code = {'auto': _lib.FORM_AUTO, 'fft32': _lib.FORM_FFT32, 'tc': _lib.FORM_TC}.get(form)
         if code is None:
             raise ValueError(f'framecor: unknown form {form}')
         _lib.raise_for(_lib.lib().b200_set_form(self._h, code), self._h)
