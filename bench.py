@@ -44,6 +44,15 @@ def fft_flops(n):
     return 2 * 2.5 * n * n * np.log2(n * n) + 6 * n * (n // 2 + 1)
 
 
+def tc_flops(n, m):
+    """executed tensor-core FLOPs of one window in the DFT-GEMM form (FFT size n, m shifts per
+    axis): the five GEMM stages with their 128-row tiles and 16-column padding"""
+    kp = (n // 2 + 1 + 15) // 16 * 16
+    no = (m + 15) // 16 * 16
+    t1 = (n + 127) // 128
+    return 4 * 128 * t1 * kp * n + 8 * 128 * n * n + 8 * 128 * no * n + 4 * 128 * no * kp
+
+
 class Clocks:
     """nvidia-smi samples of one GPU while running."""
     FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
@@ -232,6 +241,20 @@ def run_b200(args):
         ms = float(t.item())
     value = world * args.steps * BATCH * nwin / (ms / 1e3)
 
+    # the other form on the same steps (device time), for comparison
+    other = 'fft32' if args.form == 'tc' else 'tc'
+    cor.set_form(other)
+    for i in range(2):
+        step_dev(i)
+    torch.cuda.synchronize()
+    e0.record()
+    for i in range(args.steps):
+        step_dev(args.warmup + i)
+    e1.record()
+    torch.cuda.synchronize()
+    other_value = world * args.steps * BATCH * nwin / (e0.elapsed_time(e1) / 1e3)
+    cor.set_form(args.form)
+
     if args.no_e2e:
         print(json.dumps({'value': value, 'kernel_ms': kernel_ms, 'kernel_launches': kernel_launches}))
         return
@@ -277,29 +300,40 @@ def run_b200(args):
     if rank == 0:
         pk = peaks()
         sm_max = (clk or {}).get('sm_max_mhz') or pk.get('sm_max_mhz', 1965.0)
-        fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12
-        achieved = fft_flops(fft_n) * pairs / (kernel_ms / 1e3) / 1e12 if kernel_ms > 0 else None
+        if args.form == 'tc':
+            bound, peak_v = 'tensor', pk.get('bf16_tflops', 1590.0)
+            peak_src = ('measured cuBLAS bf16 burst (MEASURED_PEAKS.json)' if 'bf16_tflops' in pk
+                        else 'fallback 1.59 PFLOP/s')
+            work = tc_flops(fft_n, 2 * SEARCH + 1)
+            kname = f'corr_tc_kernel<{fft_n}>'
+        else:
+            bound, peak_v = 'fp32', 148 * 128 * 2 * sm_max * 1e6 / 1e12
+            peak_src = 'nominal FP32 CUDA-core peak: 148 SMs x 128 lanes x 2 x max SM clock'
+            work = fft_flops(fft_n)
+            kname = f'corr_kernel<{fft_n}>'
+        achieved = work * pairs / (kernel_ms / 1e3) / 1e12 if kernel_ms > 0 else None
         out = {
             'metric': METRIC, 'value': value, 'unit': 'windows/s', 'n_gpus': world, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': ms / args.steps, 'higher_is_better': True, 'scaling': 'weak',
-            'vs_baseline': value / PUBLISHED_WPS, 'dtype': 'f32', 'data': 'synthetic',
+            'vs_baseline': value / PUBLISHED_WPS, 'dtype': 'f16' if args.form == 'tc' else 'f32', 'data': 'synthetic',
             'config': {'workload': '720p video (300 frames), window 64, search 48, skip 16 (2450 windows/frame), '
                                    'per-frame gross = rounded camera motion',
                        'frames_per_step': BATCH, 'windows_per_step': BATCH * nwin, 'fft_size': fft_n,
-                       'form': 'fft32', 'parallelism': f'frames sharded over {world} GPU(s)',
+                       'form': args.form, 'parallelism': f'frames sharded over {world} GPU(s)',
                        'l2': 'per step: 254 MB of resident reference spectra + 14.7 MB of frames read '
                              '(> 126 MB L2); the batches walk through a 276 MB video'},
             'e2e': {'value': e2e, 'unit': 'windows/s', 'h2d_bytes_per_step': BATCH * H * W_ + BATCH * 2 * 4,
                     'd2h_bytes_per_step': BATCH * nwin * 7 * 4},
             'gpu_launches': launches,
-            'roofline': {'bound': 'fp32', 'achieved': achieved, 'peak': fp32_peak, 'unit': 'TFLOP/s',
-                         'frac': (achieved / fp32_peak) if achieved else None,
-                         'traffic': profiled_traffic('fft32', fft_n) if BATCH == 16 else None,
+            'roofline': {'bound': bound, 'achieved': achieved, 'peak': peak_v, 'unit': 'TFLOP/s',
+                         'frac': (achieved / peak_v) if achieved else None,
+                         'traffic': profiled_traffic(args.form, fft_n) if BATCH == 16 else None,
                          'traffic_source': 'ncu dram__bytes_read.sum + dram__bytes_write.sum of one 16-frame launch '
-                                           '(profiles/corr_fft32_720p_w64_s48.md)',
-                         'kernel': 'corr_kernel<160>', 'kernel_ms_per_launch': kernel_ms / max(kernel_launches, 1),
-                         'peak_source': 'nominal FP32 CUDA-core peak: 148 SMs x 128 lanes x 2 x max SM clock',
-                         'flop_per_window': fft_flops(fft_n)},
+                                           f'(profiles/corr_{args.form}_720p_w64_s48.md)',
+                         'kernel': kname, 'kernel_ms_per_launch': kernel_ms / max(kernel_launches, 1),
+                         'peak_source': peak_src, 'flop_per_window': work,
+                         'useful_fft_flop_per_window': fft_flops(fft_n)},
+            'other_form': {'form': other, 'value': other_value, 'unit': 'windows/s'},
             'accuracy': None if err is None else {'vs': 'FP64 direct-correlation oracle, 2 frames, 7 x 10 windows',
                                                   'median_px': err[0], 'p99_px': err[1], 'frac_above_0.01px': err[2]},
             'clocks': clk,
@@ -324,7 +358,7 @@ def main():
     p.add_argument('--no-e2e', action='store_true', help='device timing only (profiling runs)')
     p.add_argument('--video', type=int, default=NFRAMES, help='frames of the synthetic video to render')
     p.add_argument('--batch', type=int, default=BATCH, help='frames per step')
-    p.add_argument('--form', default='fft32', choices=['fft32', 'tc'], help='the arithmetic of the transforms')
+    p.add_argument('--form', default='tc', choices=['fft32', 'tc'], help='the arithmetic of the transforms')
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == 'reference':

@@ -267,6 +267,7 @@ struct b200_handle {
     DevBuf<int> d_down, d_across;
     DevBuf<float> d_norm;
     DevBuf<float2> d_spec, d_tw;
+    DevBuf<float4> d_spec_tc;    // the reference spectra in the tensor-core form's order
     DevBuf<uint8_t> d_ref;
     DevBuf<uint32_t> d_sat;      // device-path scratch
     DevBuf<int64_t> d_sat2;
@@ -331,6 +332,7 @@ struct b200_handle {
         a.across = d_across.p;
         a.norm = d_norm.p;
         a.spec = d_spec.p;
+        a.spec_tc = d_spec_tc.p;
         a.twiddles = d_tw.p;
         a.gross = gross;
         a.gross_mode = gross_mode;
@@ -435,6 +437,11 @@ void upload_reference(b200_handle *h, const uint8_t *dframe, int pitch, cudaStre
     B200_DISPATCH(h->N, launch_spectra, a, h->nwin, s);
     CK(cudaGetLastError());
     h->launches += 1;
+    if (h->tc_ok) {
+        spec_tc_kernel<<<unsigned(4 * num_sms()), 256, 0, s>>>(h->d_spec.p, h->d_spec_tc.p, h->N, h->nwin);
+        CK(cudaGetLastError());
+        h->launches += 1;
+    }
 }
 
 }   // namespace
@@ -509,6 +516,7 @@ int b200_create(const b200_params *p, int device, b200_handle **out)
             std::vector<uint16_t> dt(2 * size_t(N) * N);
             tc_dft_table(N, dt.data());
             h->d_dtab.alloc(dt.size());
+            h->d_spec_tc.alloc(size_t(h->nwin) * (N / 2) * tc_kp(N));
             CK(cudaMemcpy(h->d_dtab.p, dt.data(), dt.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
         }
         const size_t G = size_t(h->group), P = G * h->nwin;
@@ -812,6 +820,7 @@ int b200_correlate_device_noalloc(b200_handle *h, const uint8_t *frames, int n, 
             a.across = h->d_across.p;
             a.norm = h->d_norm.p;
             a.spec = h->d_spec.p;
+            a.spec_tc = h->d_spec_tc.p;
             a.twiddles = h->d_tw.p;
             a.gross = gross_mode == B200_GROSS_FRAME ? gross + 2 * size_t(f0)
                     : gross_mode == B200_GROSS_WINDOW ? gross + 2 * q0 : nullptr;

@@ -56,6 +56,7 @@ struct CorrArgs {
     const int *down, *across;
     const float *norm;         // nwin
     const float2 *spec;        // the reference spectra
+    const float4 *spec_tc;     // the same, in the order the tensor-core form reads them (or nullptr)
     const float2 *twiddles;    // 2N
     const int32_t *gross;      // nullptr, nf x 2 (per frame) or nf x nwin x 2 (per window)
     int gross_mode;            // 0 none, 1 per frame, 2 per window

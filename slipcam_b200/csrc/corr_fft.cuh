@@ -26,21 +26,22 @@ B200_HD double parabola64(double m, double c, double p)
     return den < 0 ? 0.5 * (m - p) / den : 0.0;
 }
 
-// The outputs of pair q from its normalized surface s (float, row pitch `pitch`) and its peak
-// (u, v), following cxx/surface.h:71-146: the 3 x 3 quadratic fit (else a parabola per axis; no
+// The outputs of pair q from its normalized surface around the peak (u, v) -- c points at the
+// peak's value, rows `pitch` floats apart; only c's 3 x 3 neighbourhood is read, and only when
+// the peak is not on the edge -- following cxx/surface.h:71-146: the 3 x 3 quadratic fit (else a parabola per axis; no
 // sub-pixel at the edge), solved in FP64; the SNR from snr_sum, the sum of the squared surface
 // over the stat patch clipped to the surface, and its count; the covariance from the curvature.
-B200_HD void peak_outputs(const float *s, int pitch, int M, int u, int v, int R, int gy, int gx,
+B200_HD void peak_outputs(const float *c, int pitch, int M, int u, int v, int R, int gy, int gx,
                           int tsize, double snr_sum, int snr_count, int64_t q, float *offset,
                           float *peak, float *snr, float *cov)
 {
-    const double f0 = s[u * pitch + v];
+    const double f0 = c[0];
     const bool inside = u > 0 && u < M - 1 && v > 0 && v < M - 1;
     double du = 0.0, dv = 0.0;
     if (inside) {
         double f[3][3];
         for (int i = 0; i < 3; i++)
-            for (int j = 0; j < 3; j++) f[i][j] = s[(u + i - 1) * pitch + v + j - 1];
+            for (int j = 0; j < 3; j++) f[i][j] = c[(i - 1) * pitch + j - 1];
         constexpr double sixth = 1.0 / 6.0;   // the surface.h divisions by 6 and 4, as products
         const double c1 = (f[2][0] + f[2][1] + f[2][2] - f[0][0] - f[0][1] - f[0][2]) * sixth;
         const double c2 = (f[0][2] + f[1][2] + f[2][2] - f[0][0] - f[1][0] - f[2][0]) * sixth;
@@ -71,10 +72,9 @@ B200_HD void peak_outputs(const float *s, int pitch, int M, int u, int v, int R,
     cov[3 * q + 2] = 0.0f;
     if (inside) {
         const double T = tsize;
-        const double dxx = -(s[(u + 1) * pitch + v] + s[(u - 1) * pitch + v] - 2.0 * f0) * T;
-        const double dyy = -(s[u * pitch + v + 1] + s[u * pitch + v - 1] - 2.0 * f0) * T;
-        const double dxy = (double(s[(u + 1) * pitch + v + 1]) + s[(u - 1) * pitch + v - 1]
-                            - s[(u + 1) * pitch + v - 1] - s[(u - 1) * pitch + v + 1]) * 0.25 * T;
+        const double dxx = -(c[pitch] + c[-pitch] - 2.0 * f0) * T;
+        const double dyy = -(c[1] + c[-1] - 2.0 * f0) * T;
+        const double dxy = (double(c[pitch + 1]) + c[-pitch - 1] - c[pitch - 1] - c[-pitch + 1]) * 0.25 * T;
         double n2 = 1.0 - f0 > 0 ? 1.0 - f0 : 0.0;
         const double n4 = n2 * n2 * 0.5 * T;
         n2 *= 2;
@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(NT, (N <= 160 ? 2 : 1)) corr_kernel(CorrArgs a
     }
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
     if (lane == 0)
-        peak_outputs(Sr, G::RP, M, u, v, R, gy, gx, a.W * a.W, sum, cnt, q, a.offset, a.peak, a.snr, a.cov);
+        peak_outputs(Sr + size_t(u) * G::RP + v, G::RP, M, u, v, R, gy, gx, a.W * a.W, sum, cnt, q, a.offset, a.peak, a.snr, a.cov);
 }
 
 #endif   // __CUDACC__

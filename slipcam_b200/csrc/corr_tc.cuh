@@ -28,10 +28,13 @@ namespace b200 {
 
 constexpr uint32_t cmax(uint32_t a, uint32_t b) { return a > b ? a : b; }
 
+// the frequency rows kappa of a real N-point row transform (N / 2 + 1), padded to 16
+__host__ __device__ constexpr int tc_kp(int N) { return (N / 2 + 1 + 15) / 16 * 16; }
+
 template <int N>
 struct TcGeo {
     static constexpr int NH = N / 2 + 1;                            // frequencies of a real row
-    static constexpr int KP = (NH + 15) / 16 * 16;                  // kappa rows, padded
+    static constexpr int KP = tc_kp(N);                             // kappa rows, padded
     static constexpr int T1 = (N + 127) / 128;                      // row tiles of S1
     static constexpr uint32_t SBO_D = uint32_t(N / 8) * 128u;       // Dr, Di, X: K-major rows of N
     static constexpr uint32_t SBO_A = uint32_t(2 * N / 8) * 128u;   // A2 (MN-major), A4 (K-major): K = 2N
@@ -109,6 +112,15 @@ __device__ __forceinline__ void tc_publish()
     tc::fence_after_sync();
 }
 
+// one (window, frame) pair of the tensor-core kernel, as one thread works it out ahead of time
+struct PairSetup {
+    int64_t q;              // the output index f * nwin + k
+    int p, k, f, gy, gx;    // pair, window, frame, gross offset
+    int sy, sx, mean;       // the chip's top-left corner and its rounded mean
+    float norm;
+    bool ok;                // the chip lies inside the frame and the reference window has texture
+};
+
 // two warps per TMEM lane quadrant: warp w and w + 4 own the same 32 accumulator rows and split
 // their columns
 constexpr int kTcThreads = 256;
@@ -125,11 +137,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
 {
     using G = TcGeo<N>;
     constexpr int NH = G::NH, KP = G::KP, NT = kTcThreads;
+    constexpr bool kPeakInS3 = KP <= 3 * 32;   // TMEM lanes 96 .. 127 (the last warp's) hold no kappa row
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ uint32_t tmem_base;
     __shared__ __align__(8) uint64_t mbar, tbar;
     __shared__ float s_best[NT / 32];
     __shared__ int s_at[NT / 32];
+    __shared__ double s_sq[NT / 32];
+    __shared__ float s_fit[9];
+    __shared__ PairSetup s_next;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int quad = warp & 3, half = warp >> 2;
     const int row = 32 * quad + lane;   // this thread's accumulator row (TMEM lane)
@@ -166,8 +182,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
     const size_t ss = size_t(a.w) + 1;
     const bool words = ((a.pitch | reinterpret_cast<uintptr_t>(a.frames) | int(a.fstride)) & 3) == 0;
 
-    // the pair whose peak warp 0 still has to write: the surface stays in the A region until the
-    // next pair's first drain, after the gather
+    // the pair whose peak the last warp still has to write, from its 3 x 3 neighbourhood (s_fit) and
+    // the SNR patch's sums of squares (s_sq, one per warp), in the next pair's S3 (where the last
+    // warp has no kappa rows) or else its S1
     struct Pending {
         int64_t q;
         int at, gy, gx;
@@ -176,52 +193,71 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
     auto finish_peak = [&](Pending &pp) {
         if (!pp.live) return;
         pp.live = false;
+        if (lane != 0) return;
         if (!pp.valid) {
-            if (lane == 0) invalid_outputs(pp.q, a.offset, a.peak, a.snr, a.cov);
+            invalid_outputs(pp.q, a.offset, a.peak, a.snr, a.cov);
             return;
         }
         const int u = pp.at / M, v = pp.at % M;
         int i0, i1, j0, j1;
         snr_patch(M, a.stat, u, v, i0, i1, j0, j1);
-        const int pw = j1 - j0, cnt = (i1 - i0) * pw;
         double sum = 0.0;
-        for (int t = lane; t < cnt; t += 32) {
-            const double c = surf[(i0 + t / pw) * M + j0 + t % pw];
-            sum += c * c;
-        }
-        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-        if (lane == 0) peak_outputs(surf, M, M, u, v, R, pp.gy, pp.gx, W * W, sum, cnt, pp.q, a.offset, a.peak, a.snr, a.cov);
+        for (int w = 0; w < NT / 32; ++w) sum += s_sq[w];
+        peak_outputs(s_fit + 4, 3, M, u, v, R, pp.gy, pp.gx, W * W, sum, (i1 - i0) * (j1 - j0), pp.q, a.offset, a.peak,
+                     a.snr, a.cov);
     };
 
-    for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
-        if (warp == 0) finish_peak(pend);
-        const int k = p / a.nf, f = p % a.nf;
-        const int64_t q = int64_t(f) * a.nwin + k;
-        int gy = 0, gx = 0;
+    // the next pair's window, frame, position and chip mean, worked out by one thread of the last
+    // warp while the tensor cores run S2 (global-memory latency off the gather's path)
+    auto pair_setup = [&](int p) {
+        PairSetup o{};
+        o.p = p;
+        if (p >= npairs) return o;
+        o.k = p / a.nf;
+        o.f = p % a.nf;
+        o.q = int64_t(o.f) * a.nwin + o.k;
         if (a.gross_mode == 1) {
-            gy = a.gross[2 * f];
-            gx = a.gross[2 * f + 1];
+            o.gy = a.gross[2 * o.f];
+            o.gx = a.gross[2 * o.f + 1];
         } else if (a.gross_mode == 2) {
-            gy = a.gross[2 * q];
-            gx = a.gross[2 * q + 1];
+            o.gy = a.gross[2 * o.q];
+            o.gx = a.gross[2 * o.q + 1];
         }
-        const int sy = a.down[k / a.nx] + gy - R, sx = a.across[k % a.nx] + gx - R;
-        const float norm = a.norm[k];
-        if (!(norm > 0) || sy < 0 || sx < 0 || sy + L > a.h || sx + L > a.w) {
+        o.sy = a.down[o.k / a.nx] + o.gy - R;
+        o.sx = a.across[o.k % a.nx] + o.gx - R;
+        o.norm = a.norm[o.k];
+        o.ok = o.norm > 0 && o.sy >= 0 && o.sx >= 0 && o.sy + L <= a.h && o.sx + L <= a.w;
+        if (o.ok) {
+            const uint32_t *sat = a.sat + size_t(o.f) * a.sat_fstride;
+            const int sy = o.sy, sx = o.sx;
+            const uint32_t box = sat[(sy + L) * ss + sx + L] - sat[sy * ss + sx + L] - sat[(sy + L) * ss + sx] + sat[sy * ss + sx];
+            const uint32_t LL = uint32_t(L) * uint32_t(L);
+            o.mean = int((box + LL / 2) / LL);
+        }
+        return o;
+    };
+    if (tid == NT - 32) s_next = pair_setup(blockIdx.x);
+    __syncthreads();
+
+    for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
+        const PairSetup cur = s_next;
+        const int k = cur.k, f = cur.f, sy = cur.sy, sx = cur.sx;
+        const int64_t q = cur.q;
+        const float norm = cur.norm;
+        if (!cur.ok) {
             if (tid == 0) invalid_outputs(q, a.offset, a.peak, a.snr, a.cov);
             if (a.surface)
                 for (int i = tid; i < M * M; i += NT) a.surface[q * M * M + i] = 0.0f;
+            __syncthreads();   // every thread has read s_next
+            if (tid == NT - 32) s_next = pair_setup(p + gridDim.x);
+            __syncthreads();
             continue;
         }
 
         // ---- X = chip - round(mean), FP16, K-major (rows i, columns j), zero outside L x L. A warp
         // takes 8 rows x 4 chunks of 8 pixels: 32-byte pieces of 8 rows from global memory, one
         // contiguous 512-byte store into shared memory. Every load of the thread first.
-        const uint32_t *sat = a.sat + size_t(f) * a.sat_fstride;
-        const uint32_t box = sat[(sy + L) * ss + sx + L] - sat[sy * ss + sx + L] - sat[(sy + L) * ss + sx] + sat[sy * ss + sx];
-        const uint32_t LL = uint32_t(L) * uint32_t(L);
-        const int mean = int((box + LL / 2) / LL);
-        const __half2 off = __float2half2_rn(1024.0f + float(mean));
+        const __half2 off = __float2half2_rn(1024.0f + float(cur.mean));
         const uint8_t *chip = a.frames + f * a.fstride + int64_t(sy) * a.pitch + sx;
         {
             constexpr int NCG = (N / 8 + 3) / 4;               // groups of 4 chunks per row
@@ -303,6 +339,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
             }
             tc::mma_commit(&mbar);
         }
+        if (!kPeakInS3 && warp == NT / 32 - 1) finish_peak(pend);   // the previous pair's peak, while S1 runs
         if (!tc_wait_all(&mbar, phase)) {
             if (tid == 0 && status) atomicExch(status, 3);
             break;
@@ -346,11 +383,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
             tc::mbar_expect_tx(&tbar, uint32_t(BW * M * 4));
             tc::tma_load_3d(dvs, dmap, sx & ~3, sy, f, &tbar);
         }
-        // and this thread's row of the reference spectrum (S3)
+        if (tid == NT - 32) s_next = pair_setup(p + gridDim.x);   // read after S2's barrier
+        // and this thread's row of the reference spectrum (S3): frequency pairs (ky, ky + 1) of the
+        // rows kappa side by side, KP float4 per pair (rows NH .. KP - 1 zero)
         int eR = 0;
         frexpf(float(W) * norm, &eR);   // W * norm < 2^eR, and max |R| <= W * norm
         const int kap = row;
-        const float4 *rrow = reinterpret_cast<const float4 *>(a.spec + (size_t(k) * NH + (kap < NH ? kap : 0)) * N);
+        const float4 *rrow = a.spec_tc + size_t(k) * (N / 2) * KP + (kap < KP ? kap : 0);
         if (!tc_wait_all(&mbar, phase)) {
             if (tid == 0 && status) atomicExch(status, 3);
             break;
@@ -362,7 +401,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
             const float sc = ldexpf(1.0f, -(eR + 8));
             float4 rn[8];
 #pragma unroll
-            for (int e = 0; e < 8; ++e) rn[e] = kap < NH ? __ldg(rrow + 8 * half + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int e = 0; e < 8; ++e) rn[e] = kap < KP ? __ldg(rrow + (8 * half + e) * KP) : make_float4(0.f, 0.f, 0.f, 0.f);
             for (int c0 = 16 * half; c0 < N; c0 += 32) {
                 uint32_t zr[16], zi[16];
                 tc::tmem_ld16_nowait(tmem + lane_base + uint32_t(c0), zr);
@@ -370,9 +409,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
                 float4 rc[8];
 #pragma unroll
                 for (int e = 0; e < 8; ++e) rc[e] = rn[e];
-                if (c0 + 32 < N && kap < NH) {
+                if (c0 + 32 < N && kap < KP) {
 #pragma unroll
-                    for (int e = 0; e < 8; ++e) rn[e] = __ldg(rrow + (c0 + 32) / 2 + e);
+                    for (int e = 0; e < 8; ++e) rn[e] = __ldg(rrow + ((c0 + 32) / 2 + e) * KP);
                 }
                 tc::tmem_wait();
                 if (kap < KP) {
@@ -395,6 +434,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
                     }
                 }
             }
+        } else if (kPeakInS3 && warp == NT / 32 - 1) {
+            finish_peak(pend);   // the previous pair's peak
         }
         tc_publish();
 
@@ -466,25 +507,31 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
         int at = INT_MAX;
         if (32 * quad < M) {
             const int v = row;
+            const bool vin = v < M;
             const float *__restrict__ dv = dvs + (sx & 3) + v;
             float *__restrict__ sv = surf + v;
             for (int u0 = 16 * half; u0 < NO; u0 += 32) {   // one 16-column chunk of u per TMEM wait
                 uint32_t cr[16];
                 tc::tmem_ld16_nowait(tmem + lane_base + uint32_t(u0), cr);
-                tc::tmem_wait();
-                if (v < M) {
+                const int nu = M - u0 < 16 ? M - u0 : 16;   // rows u of the chunk inside the surface
+                float rho[16];
 #pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        const int u = u0 + e;
-                        if (u < M) {
-                            const float rho = __uint_as_float(cr[e]) * scale * dv[u * BW];
-                            sv[u * M] = rho;
-                            if (rho > best) {
-                                best = rho;
-                                at = u;
-                            }
+                for (int e = 0; e < 16; ++e) rho[e] = vin && e < nu ? dv[(u0 + e) * BW] : 0.0f;
+                tc::tmem_wait();
+#pragma unroll
+                for (int e = 0; e < 16; ++e) rho[e] *= __uint_as_float(cr[e]) * scale;
+                if (vin) {
+#pragma unroll
+                    for (int e = 0; e < 16; ++e)
+                        if (e < nu) sv[(u0 + e) * M] = rho[e];
+                }
+                if (vin) {
+#pragma unroll
+                    for (int e = 0; e < 16; ++e)   // values <= -2 and NaN never win; ties keep the first u
+                        if (e < nu && rho[e] > best) {
+                            best = rho[e];
+                            at = u0 + e;
                         }
-                    }
                 }
             }
             at = at == INT_MAX ? INT_MAX : at * M + v;
@@ -498,20 +545,57 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
         __syncthreads();
         if (a.surface)
             for (int i = tid; i < M * M; i += NT) a.surface[q * M * M + i] = surf[i];
-        if (warp == 0) {
-            best = lane < NT / 32 ? s_best[lane] : -2.0f;
-            at = lane < NT / 32 ? s_at[lane] : INT_MAX;
-            for (int o = 16; o > 0; o >>= 1) better(best, at, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, at, o));
-            pend = {q, at, gy, gx, best > 0, true};   // finished while the next chip loads
+        // every warp: the argmax of the surface, then its rows of the SNR patch's sum of squares
+        best = lane < NT / 32 ? s_best[lane] : -2.0f;
+        at = lane < NT / 32 ? s_at[lane] : INT_MAX;
+        for (int o = 16; o > 0; o >>= 1) better(best, at, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, at, o));
+        double sq = 0.0;
+        if (best > 0) {
+            const int pu = at / M, pv = at % M;
+            if (tid < 9 && pu > 0 && pu < M - 1 && pv > 0 && pv < M - 1)
+                s_fit[tid] = surf[(pu + tid / 3 - 1) * M + pv + tid % 3 - 1];   // the 3 x 3 fit's values
+            else if (tid == 0)
+                s_fit[4] = surf[pu * M + pv];
+            int i0, i1, j0, j1;
+            snr_patch(M, a.stat, pu, pv, i0, i1, j0, j1);
+            for (int i = i0 + warp; i < i1; i += NT / 32)
+                for (int j = j0 + lane; j < j1; j += 32) {
+                    const double c = surf[i * M + j];
+                    sq += c * c;
+                }
         }
+        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+        if (lane == 0) s_sq[warp] = sq;
+        pend = {q, at, cur.gy, cur.gx, best > 0, true};
         __syncthreads();
         tc::fence_after_sync();
     }
-    if (warp == 0) finish_peak(pend);
+    if (warp == NT / 32 - 1) finish_peak(pend);
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) tc::tmem_dealloc(tmem, G::TMEM_COLS);
 #undef B200_TC_DESCS
+}
+
+// the reference spectra in the order S3 of the tensor-core form reads them: for window k and the
+// frequency pair (ky, ky + 1) = (2 p, 2 p + 1), the rows kappa < KP side by side, one float4
+// (R[kappa][2 p], R[kappa][2 p + 1]) each, rows NH .. KP - 1 zero. spec holds nwin x NH x N.
+__global__ void spec_tc_kernel(const float2 *__restrict__ spec, float4 *__restrict__ out, int N, int nwin)
+{
+    const int NH = N / 2 + 1, KP = tc_kp(N);
+    const int64_t total = int64_t(nwin) * (N / 2) * KP;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
+        const int kap = int(i % KP);
+        const int64_t kp = i / KP;
+        const int pr = int(kp % (N / 2));
+        const int64_t k = kp / (N / 2);
+        float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (kap < NH) {
+            const float2 *r = spec + (k * NH + kap) * N + 2 * pr;
+            o = make_float4(r[0].x, r[0].y, r[1].x, r[1].y);
+        }
+        out[i] = o;
+    }
 }
 
 #endif   // __CUDACC__

@@ -190,3 +190,70 @@ def test_hd_recovers_motion():
     for k in range(2):
         err = off[k] - motion[k + 1][None, None, :]
         assert np.nanmedian(np.abs(err)) < 0.05
+
+
+# ---- the tensor-core form (FP16 operands, FP32 accumulation). At the 720p geometry (W64, R48) it
+# holds the FP32 form's gates: offsets within 0.01 px and SNR within 1e-3 of the FP64 oracle. With
+# smaller windows the FP16 surface error (~3e-4) flips the reference's piecewise sub-pixel estimator
+# (3 x 3 fit or per-axis parabola) for some windows near a branch boundary and moves the SNR of
+# clean, sharp peaks (small patch sums): there the typical error stays below 2e-3 px and at most 5 %
+# of the pairs (2 in a small case) may exceed 0.01 px, none by more than 0.1 px.
+TC_CASES = ['shifts', 'gross', 'window_gross', 'invalid', 'small', 'hd', 'mixed']
+
+
+@pytest.mark.parametrize('name', TC_CASES)
+def test_tc_fp64_oracle(name):
+    c = cases.case(name)
+    cor = framecor.Correlator(c['height'], c['width'], c['down'], c['across'], window=c['window'],
+                              search=c['search'], stat_size=c['stat_size'], backend='b200')
+    cor.set_form('tc')
+    cor.set_reference(c['reference'])
+    r = cor.correlate(c['frames'], gross=c['gross'])
+    down, across, gross = c['down'], c['across'], c['gross']
+    sl = (slice(None), slice(None, None, 7), slice(None, None, 9)) if name == 'hd' else (slice(None),) * 3
+    if name == 'hd':
+        down, across = down[::7], across[::9]
+    o = oracle.correlate(c['height'], c['width'], down, across, c['reference'], c['frames'],
+                         gross if gross is None or gross.ndim == 2 else gross[sl], window=c['window'],
+                         search=c['search'], stat_size=c['stat_size'], mode='f64')
+    b = {k: v[sl] for k, v in r.items()}
+    assert np.array_equal(np.isnan(o['offsets']), np.isnan(b['offsets']))
+    valid = np.isfinite(o['offsets'][..., 0])
+    assert np.all(b['cov'][~valid] == np.array([99, 99, 0], np.float32))
+    d = np.abs(o['offsets64'] - b['offsets']).max(-1)
+    mism = valid & (d > 0.5)
+    assert mism.sum() <= max(1, int(valid.sum() * TIE_SHARE.get(name, 0.01)))
+    ok = valid & ~mism
+    assert np.abs(b['peak'][ok] - o['peak'][ok]).max() < 1e-3
+    snr_rel = np.abs(b['snr'][ok] / o['snr'][ok] - 1)
+    if name == 'hd':
+        assert d[ok].max() < 0.01, d[ok].max()
+        assert snr_rel.max() < 1e-3, snr_rel.max()
+    else:
+        assert np.median(d[ok]) < 2e-3
+        assert (d[ok] > 0.01).sum() <= max(2, 0.05 * ok.sum())
+        assert d[ok].max() < 0.1
+        assert np.median(snr_rel) < 1e-3
+
+
+def test_tc_surfaces_close_to_fft32():
+    c = cases.case('hd')
+    cor = framecor.Correlator(c['height'], c['width'], c['down'], c['across'], window=64, search=48, backend='b200')
+    cor.set_reference(c['reference'])
+    f = torch.as_tensor(c['frames']).cuda()
+    g = torch.as_tensor(c['gross']).cuda()
+    s32 = cor.correlate(f, gross=g, surfaces=True)['surface']
+    cor.set_form('tc')
+    stc = cor.correlate(f, gross=g, surfaces=True)['surface']
+    assert torch.isfinite(stc).all()
+    assert (stc - s32).abs().max().item() < 2e-3
+
+
+def test_tc_form_limits():
+    """Geometries the tensor-core kernel does not hold are refused with a ValueError."""
+    down, across = framecor.window_grid(512, 512, 64, 64, 64)   # L = 192
+    cor = framecor.Correlator(512, 512, down, across, window=64, search=64, backend='b200')
+    with pytest.raises(ValueError, match='tensor-core'):
+        cor.set_form('tc')
+    with pytest.raises(ValueError):
+        cor.set_form('bf16')
