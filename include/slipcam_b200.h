@@ -125,6 +125,41 @@ B200_API int b200_correlate_device_noalloc(b200_handle *h, const uint8_t *frames
                                            const int32_t *gross, int gross_mode, float *offset,
                                            float *peak, float *snr, float *cov, void *stream);
 
+/* ---- The differentiable path: float frames, a continuous shift per pair, and the adjoints.
+ * No counterpart in the reference (its backends take uint8 frames and give no derivatives); the
+ * math follows the same correlation (cxx/cpu.cpp:115-160, cxx/surface.h:30-146) and is stated in
+ * slipcam_b200/csrc/diff.h. All pointers are device memory, stream-ordered on `stream`.
+ *
+ * b200_set_reference_f32_device: the reference windows and spectra from a float32 frame (rows
+ * `pitch` floats apart), as b200_set_reference_device does from a uint8 frame. */
+B200_API int b200_set_reference_f32_device(b200_handle *h, const float *frame, int pitch, void *stream);
+
+/* The forward pass over n float32 frames (rows `pitch` floats apart, frames pitch * height
+ * floats apart). shift: NULL or n x nwin x 2 floats (ty, tx), a continuous shift of each pair's
+ * search window, sampled with Keys' six-point cubic convolution (the edge pixel repeats beyond
+ * the frame); a pair is invalid as in the reference, at the floored position of its shifted
+ * window (cxx/surface.h:39-45). Writes chips (n x nwin x L x L),
+ * stats (n x nwin x M x M x 2: the box mean and 1 / sqrt(n var)), surface (n x nwin x M x M),
+ * peak_at (n x nwin: u M + v, -1 if invalid) and the reference's four outputs (the offsets
+ * without the shift: the caller adds it). L = window + 2 search, M = 2 search + 1. */
+B200_API int b200_diff_forward(b200_handle *h, const float *frames, int n, int pitch, const int32_t *gross,
+                               int gross_mode, const float *shift, float *chips, float *stats, float *surface,
+                               int *peak_at, float *offset, float *peak, float *snr, float *cov, void *stream);
+
+/* The backward pass: from g_surface (n x nwin x M x M) and the forward's chips, stats and
+ * surface, the chip cotangents g_chips (n x nwin x L x L, written), the frame cotangents g_frames
+ * (n x height x pitch floats, accumulated into: zero it first; NULL to skip) and the shift
+ * cotangents g_shift (n x nwin x 2, written; NULL to skip). */
+B200_API int b200_diff_backward(b200_handle *h, const float *frames, int n, int pitch, const int32_t *gross,
+                                int gross_mode, const float *shift, const float *chips, const float *stats,
+                                const float *surface, const float *g_surface, float *g_chips, float *g_frames,
+                                float *g_shift, void *stream);
+
+/* The surface cotangent of the sub-pixel offsets: g_surface (n x nwin x M x M, zeroed here) from
+ * g_offset (n x nwin x 2) through the branch of the 3 x 3 fit each pair's peak took. */
+B200_API int b200_offset_adjoint(b200_handle *h, int n, const float *surface, const int *peak_at,
+                                 const float *g_offset, float *g_surface, void *stream);
+
 /* The summed-area tables of n frames on the device (cxx/cpu.cpp:24-42, cxx/cuda.cu:72-110):
  * sat (uint32, exact modulo 2^32) and sat2 (int64), each n x (height + 1) x (width + 1). */
 B200_API int b200_sat_device(const uint8_t *frames, int n, int height, int width, int pitch, uint32_t *sat,

@@ -34,6 +34,10 @@ SIGNATURES = {
     'b200_correlate_device': (_i, [_vp, _u8p, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp]),
     'b200_correlate_device_surfaces': (_i, [_vp, _u8p, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
     'b200_correlate_device_noalloc': (_i, [_vp, _u8p, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp]),
+    'b200_set_reference_f32_device': (_i, [_vp, _vp, _i, _vp]),
+    'b200_diff_forward': (_i, [_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    'b200_diff_backward': (_i, [_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    'b200_offset_adjoint': (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
     'b200_sat_device': (_i, [_u8p, _i, _i, _i, _i, _vp, _vp, _vp]),
     'b200_set_form': (_i, [_vp, _i]),
     'b200_tc_selftest': (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _vp]),

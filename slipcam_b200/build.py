@@ -11,11 +11,11 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, 'csrc')
 LIB = os.path.join(HERE, 'libslipcam_b200.so')
-SOURCES = ['capi.cu']
+SOURCES = ['capi.cu', 'diff.cu']
 NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 FLAGS = ['-std=c++17', '-O3', '--expt-relaxed-constexpr', '-gencode', 'arch=compute_100a,code=sm_100a',
-         '-lineinfo', '-Xcompiler', '-fPIC', '-Xcompiler', '-fvisibility=hidden', '-shared',
-         '-cudart', 'static', '-diag-suppress', '20014']
+         '-lineinfo', '-Xcompiler', '-fPIC', '-Xcompiler', '-fvisibility=hidden', '-diag-suppress', '20014']
+LINK = ['-gencode', 'arch=compute_100a,code=sm_100a', '-shared', '-cudart', 'static']
 
 
 def _stale():
@@ -31,10 +31,24 @@ def build(force=False, verbose=False):
     """Compile the library if a source is newer than it (or force); returns its path."""
     if not force and not _stale():
         return LIB
-    cmd = [NVCC, *FLAGS, *[os.path.join(CSRC, s) for s in SOURCES], '-o', LIB + '.tmp']
+    # one object per source, compiled side by side, then one link
+    objs, procs = [], []
+    for src in SOURCES:
+        obj = os.path.join(CSRC, os.path.splitext(src)[0] + '.o')
+        cmd = [NVCC, *FLAGS, '-c', os.path.join(CSRC, src), '-o', obj]
+        if verbose:
+            print(' '.join(cmd), flush=True)
+        objs.append(obj)
+        procs.append(subprocess.Popen(cmd))
+    failed = [p.args for p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
+    cmd = [NVCC, *LINK, *objs, '-o', LIB + '.tmp']
     if verbose:
         print(' '.join(cmd), flush=True)
     subprocess.run(cmd, check=True)
+    for obj in objs:
+        os.remove(obj)
     os.replace(LIB + '.tmp', LIB)
     return LIB
 

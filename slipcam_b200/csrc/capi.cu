@@ -22,6 +22,7 @@
 #include "../../include/slipcam_b200.h"
 #include "corr_fft.cuh"
 #include "corr_tc.cuh"
+#include "diff.h"
 #include "sat.cuh"
 #include "tc_selftest.cuh"
 
@@ -422,10 +423,11 @@ int guarded(b200_handle *h, F &&f)
     }
 }
 
-void upload_reference(b200_handle *h, const uint8_t *dframe, int pitch, cudaStream_t s)
+void upload_reference(b200_handle *h, const uint8_t *dframe, int pitch, cudaStream_t s, const float *dframef = nullptr)
 {
     SpectraArgs a{};
     a.frame = dframe;
+    a.framef = dframef;
     a.pitch = pitch;
     a.W = h->W;
     a.nx = h->nx;
@@ -442,6 +444,40 @@ void upload_reference(b200_handle *h, const uint8_t *dframe, int pitch, cudaStre
         CK(cudaGetLastError());
         h->launches += 1;
     }
+}
+
+// the differentiable path's arguments for n frames (diff.h)
+DiffArgs diff_args(b200_handle *h, const float *frames, int n, int pitch, const int32_t *gross, int gross_mode,
+                   const float *shift)
+{
+    if (!h->ready) fail(B200_ERUNTIME, "set_reference first");
+    if (n < 0) fail(B200_EINVAL, "the number of frames must not be negative");
+    if (n && (!frames || pitch < h->width)) fail(B200_EINVAL, "no frames, or their pitch is below their width");
+    if (gross_mode < B200_GROSS_NONE || gross_mode > B200_GROSS_WINDOW || (gross_mode && !gross))
+        fail(B200_EINVAL, "gross must be frames x 2 or frames x down x across x 2");
+    DiffArgs a{};
+    a.frames = frames;
+    a.pitch = pitch;
+    a.fstride = int64_t(pitch) * h->height;
+    a.h = h->height;
+    a.w = h->width;
+    a.W = h->W;
+    a.R = h->R;
+    a.L = h->L;
+    a.M = h->M;
+    a.nx = h->nx;
+    a.nwin = h->nwin;
+    a.n = n;
+    a.stat = h->stat;
+    a.down = h->d_down.p;
+    a.across = h->d_across.p;
+    a.norm = h->d_norm.p;
+    a.spec = h->d_spec.p;
+    a.twiddles = h->d_tw.p;
+    a.gross = gross;
+    a.gross_mode = gross_mode;
+    a.shift = shift;
+    return a;
 }
 
 }   // namespace
@@ -855,6 +891,75 @@ int b200_tc_selftest(const void *A, const void *B, float *D, int N, int K, int a
     cudaFreeAsync(status, s);
     if (!ok) return B200_ERUNTIME;
     return h ? B200_ETIMEOUT : B200_OK;
+}
+
+int b200_set_reference_f32_device(b200_handle *h, const float *frame, int pitch, void *stream)
+{
+    return guarded(h, [&] {
+        if (!frame || pitch < h->width) fail(B200_EINVAL, "no reference frame, or its pitch is below its width");
+        CK(cudaSetDevice(h->device));
+        upload_reference(h, nullptr, pitch, static_cast<cudaStream_t>(stream), frame);
+        h->ready = true;
+    });
+}
+
+int b200_diff_forward(b200_handle *h, const float *frames, int n, int pitch, const int32_t *gross, int gross_mode,
+                      const float *shift, float *chips, float *stats, float *surface, int *peak_at, float *offset,
+                      float *peak, float *snr, float *cov, void *stream)
+{
+    return guarded(h, [&] {
+        DiffArgs a = diff_args(h, frames, n, pitch, gross, gross_mode, shift);
+        if (n == 0) return;
+        if (!chips || !stats || !surface || !peak_at || !offset || !peak || !snr || !cov) fail(B200_EINVAL, "null output");
+        a.chips = chips;
+        a.stats = stats;
+        a.surface = surface;
+        a.peak_at = peak_at;
+        a.offset = offset;
+        a.peak = peak;
+        a.snr = snr;
+        a.cov = cov;
+        CK(cudaSetDevice(h->device));
+        launch_diff_forward(a, h->N, static_cast<cudaStream_t>(stream));
+        h->launches += 3;
+    });
+}
+
+int b200_diff_backward(b200_handle *h, const float *frames, int n, int pitch, const int32_t *gross, int gross_mode,
+                       const float *shift, const float *chips, const float *stats, const float *surface,
+                       const float *g_surface, float *g_chips, float *g_frames, float *g_shift, void *stream)
+{
+    return guarded(h, [&] {
+        DiffArgs a = diff_args(h, frames, n, pitch, gross, gross_mode, shift);
+        if (n == 0) return;
+        if (!chips || !stats || !surface || !g_surface || !g_chips) fail(B200_EINVAL, "null input or output");
+        a.chips = const_cast<float *>(chips);
+        a.stats = const_cast<float *>(stats);
+        a.surface = const_cast<float *>(surface);
+        a.g_surface = g_surface;
+        a.g_chips = g_chips;
+        a.g_frames = g_frames;
+        a.g_shift = g_shift;
+        CK(cudaSetDevice(h->device));
+        launch_diff_backward(a, h->N, static_cast<cudaStream_t>(stream));
+        h->launches += 2;
+    });
+}
+
+int b200_offset_adjoint(b200_handle *h, int n, const float *surface, const int *peak_at, const float *g_offset,
+                        float *g_surface, void *stream)
+{
+    return guarded(h, [&] {
+        if (n < 0) fail(B200_EINVAL, "the number of frames must not be negative");
+        if (n == 0) return;
+        if (!surface || !peak_at || !g_offset || !g_surface) fail(B200_EINVAL, "null input or output");
+        CK(cudaSetDevice(h->device));
+        const int64_t pairs = int64_t(n) * h->nwin;
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        CK(cudaMemsetAsync(g_surface, 0, size_t(pairs) * h->M * h->M * sizeof(float), s));
+        launch_offset_adjoint(surface, peak_at, g_offset, g_surface, h->M, pairs, s);
+        h->launches += 1;
+    });
 }
 
 int b200_sat_device(const uint8_t *frames, int n, int height, int width, int pitch, uint32_t *sat, int64_t *sat2,

@@ -34,7 +34,8 @@ B200_HD int xpos(int n2, int k1) { return n2 * 16 + (k1 ^ n2); }
 // the arguments of the reference-spectra kernel
 struct SpectraArgs {
     const uint8_t *frame;      // the reference frame
-    int pitch;                 // bytes per row
+    const float *framef;       // or a float reference frame (frame is then unused)
+    int pitch;                 // elements per row
     int W, nx;
     const int *down, *across;
     float *norm;               // out: nwin norms of the zero-mean windows

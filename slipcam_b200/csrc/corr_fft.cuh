@@ -109,6 +109,60 @@ B200_HD void better(float &best, int &at, float b, int ib)
 
 #ifdef __CUDACC__
 
+// The peak of pair q's normalized M x M surface Sr (row pitch `pitch` floats) and its outputs: the
+// largest value, the first in raster order if equal (cxx/cpu.cpp:148-160), invalid unless it is
+// positive; then the SNR patch sum (warp 0) and peak_outputs. peak_at (optional) receives the
+// peak's raster index u M + v, or -1. Every thread of the block calls it (it holds a barrier).
+template <int NT>
+__device__ __forceinline__ void surface_peak(const float *Sr, int pitch, int M, int R, int stat, int gy, int gx,
+                                             int tsize, int64_t q, float *offset, float *peak, float *snr, float *cov,
+                                             int *peak_at)
+{
+    __shared__ float s_best[NT / 32];
+    __shared__ int s_at[NT / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float best = -2.0f;
+    int at = INT_MAX;
+    for (int idx = threadIdx.x; idx < M * M; idx += NT) {
+        const float c = Sr[size_t(idx / M) * pitch + idx % M];
+        if (c > best) {
+            best = c;
+            at = idx;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) better(best, at, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, at, o));
+    if (lane == 0) {
+        s_best[warp] = best;
+        s_at[warp] = at;
+    }
+    __syncthreads();
+    if (warp != 0) return;
+    best = lane < NT / 32 ? s_best[lane] : -2.0f;
+    at = lane < NT / 32 ? s_at[lane] : INT_MAX;
+    for (int o = 16; o > 0; o >>= 1) better(best, at, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, at, o));
+    if (!(best > 0)) {
+        if (lane == 0) {
+            invalid_outputs(q, offset, peak, snr, cov);
+            if (peak_at) peak_at[q] = -1;
+        }
+        return;
+    }
+    const int u = at / M, v = at % M;
+    int i0, i1, j0, j1;
+    snr_patch(M, stat, u, v, i0, i1, j0, j1);
+    const int pw = j1 - j0, cnt = (i1 - i0) * pw;
+    double sum = 0.0;
+    for (int t = lane; t < cnt; t += 32) {
+        const double c = Sr[size_t(i0 + t / pw) * pitch + j0 + t % pw];
+        sum += c * c;
+    }
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) {
+        peak_outputs(Sr + size_t(u) * pitch + v, pitch, M, u, v, R, gy, gx, tsize, sum, cnt, q, offset, peak, snr, cov);
+        if (peak_at) peak_at[q] = at;
+    }
+}
+
 // the reference spectra: one CTA per reference window. Zero-mean window (its mean in double as
 // cxx/common.cpp:30-48), its norm, and its N x N forward spectrum into spec[k].
 template <int N, int NT>
@@ -124,18 +178,33 @@ __global__ void __launch_bounds__(NT) spectra_kernel(SpectraArgs a)
     const int k = blockIdx.x, W = a.W;
     const int y0 = a.down[k / a.nx], x0 = a.across[k % a.nx];
     const uint8_t *src = a.frame + size_t(y0) * a.pitch + x0;
+    const float *srcf = a.framef ? a.framef + size_t(y0) * a.pitch + x0 : nullptr;
+    auto pixel = [&](int i, int j) { return srcf ? double(srcf[size_t(i) * a.pitch + j]) : double(src[size_t(i) * a.pitch + j]); };
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
     for (int i = threadIdx.x; i < 2 * N; i += NT) TW[i] = a.twiddles[i];
-    // the sum of the window (exact, integers)
-    long long sum = 0;
-    for (int idx = threadIdx.x; idx < W * W; idx += NT) sum += src[size_t(idx / W) * a.pitch + idx % W];
-    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    if (lane == 0) redi[warp] = sum;
-    __syncthreads();
-    sum = 0;
-    for (int i = 0; i < NT / 32; ++i) sum += redi[i];
-    const double mean = double(sum) / (double(W) * W);
+    // the sum of the window (exact, integers; in double for a float frame)
+    double mean;
+    if (!srcf) {
+        long long sum = 0;
+        for (int idx = threadIdx.x; idx < W * W; idx += NT) sum += src[size_t(idx / W) * a.pitch + idx % W];
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (lane == 0) redi[warp] = sum;
+        __syncthreads();
+        sum = 0;
+        for (int i = 0; i < NT / 32; ++i) sum += redi[i];
+        mean = double(sum) / (double(W) * W);
+    } else {
+        double sum = 0.0;
+        for (int idx = threadIdx.x; idx < W * W; idx += NT) sum += pixel(idx / W, idx % W);
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (lane == 0) red[warp] = sum;
+        __syncthreads();
+        sum = 0.0;
+        for (int i = 0; i < NT / 32; ++i) sum += red[i];
+        __syncthreads();
+        mean = sum / (double(W) * W);
+    }
     // the zero-mean window, zero-padded (rows up to the even count Wr, all N columns)
     const int Wr = (W + 1) & ~1;
     double sq = 0.0;
@@ -143,7 +212,7 @@ __global__ void __launch_bounds__(NT) spectra_kernel(SpectraArgs a)
         const int i = idx / N, j = idx % N;
         float d = 0.0f;
         if (i < W && j < W) {
-            d = float(double(src[size_t(i) * a.pitch + j]) - mean);
+            d = float(pixel(i, j) - mean);
             sq += double(d) * d;
         }
         Sr[size_t(i) * G::RP + j] = d;
@@ -172,11 +241,9 @@ __global__ void __launch_bounds__(NT, (N <= 160 ? 2 : 1)) corr_kernel(CorrArgs a
     float2 *S = reinterpret_cast<float2 *>(smem_raw);
     float2 *TW = S + size_t(N) * G::NHP, *TWI = TW + N;
     float *Sr = reinterpret_cast<float *>(S);
-    __shared__ float s_best[NT / 32];
-    __shared__ int s_at[NT / 32];
     const int k = blockIdx.x / a.nf, f = blockIdx.x % a.nf;
     const int64_t q = int64_t(f) * a.nwin + k;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int warp = threadIdx.x >> 5;
 
     int gy = 0, gx = 0;
     if (a.gross_mode == 1) {
@@ -253,42 +320,7 @@ __global__ void __launch_bounds__(NT, (N <= 160 ? 2 : 1)) corr_kernel(CorrArgs a
     if (a.surface)
         for (int i = threadIdx.x; i < M * M; i += NT) a.surface[q * M * M + i] = Sr[size_t(i / M) * G::RP + i % M];
 
-    // the peak: the largest value, the first in raster order if equal (cxx/cpu.cpp:148-160)
-    float best = -2.0f;
-    int at = INT_MAX;
-    for (int idx = threadIdx.x; idx < M * M; idx += NT) {
-        const float c = Sr[size_t(idx / M) * G::RP + idx % M];
-        if (c > best) {
-            best = c;
-            at = idx;
-        }
-    }
-    for (int o = 16; o > 0; o >>= 1) better(best, at, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, at, o));
-    if (lane == 0) {
-        s_best[warp] = best;
-        s_at[warp] = at;
-    }
-    __syncthreads();
-    if (warp != 0) return;
-    best = lane < NT / 32 ? s_best[lane] : -2.0f;
-    at = lane < NT / 32 ? s_at[lane] : INT_MAX;
-    for (int o = 16; o > 0; o >>= 1) better(best, at, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, at, o));
-    if (!(best > 0)) {
-        if (lane == 0) invalid_outputs(q, a.offset, a.peak, a.snr, a.cov);
-        return;
-    }
-    const int u = at / M, v = at % M;
-    int i0, i1, j0, j1;
-    snr_patch(M, a.stat, u, v, i0, i1, j0, j1);
-    const int pw = j1 - j0, cnt = (i1 - i0) * pw;
-    double sum = 0.0;
-    for (int t = lane; t < cnt; t += 32) {
-        const double c = Sr[size_t(i0 + t / pw) * G::RP + j0 + t % pw];
-        sum += c * c;
-    }
-    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    if (lane == 0)
-        peak_outputs(Sr + size_t(u) * G::RP + v, G::RP, M, u, v, R, gy, gx, a.W * a.W, sum, cnt, q, a.offset, a.peak, a.snr, a.cov);
+    surface_peak<NT>(Sr, G::RP, M, R, a.stat, gy, gx, a.W * a.W, q, a.offset, a.peak, a.snr, a.cov, nullptr);
 }
 
 #endif   // __CUDACC__

@@ -18,6 +18,9 @@ Workloads (sizes as named):
              stripes; grids 32/16, 64/48, 128/64 (skip 16); per-window gross U[-20, 20]
   stream     1000 x 1080 x 1920, sigma 2, noise 3 DN, a 5 Hz 4 px shake plus a random walk, a
              60 px fault step over 30 frames; window 64, search 64, skip 8
+  shifts_f32 float32 frames (default 41 x 256 x 256), sigma 2, frame k moved as a whole by a
+             continuous shift U[-3, 3] px per axis (frame 0 unmoved: the reference), optional
+             Gaussian noise, not rounded; window 64, search 8, skip 32 (the differentiable path)
 """
 
 import math
@@ -162,3 +165,19 @@ def mixed(n=64, h=720, w=1280, seed=3):
     stripes = (128 + 60 * np.sin(2 * math.pi * np.arange(256) / 8.0)).astype(np.uint8)
     frames[:, y0:y0 + 160, x0:x0 + 256] = stripes[None, None, :]
     return frames, motion
+
+
+def shifts_f32(n=41, h=256, w=256, seed=4, noise=0.0, max_shift=3.0):
+    """Float frames moved by continuous shifts: frames (n, h, w) float32, shifts (n, 2) float64
+    (down, across; shifts[0] = 0). Noise (DN, Gaussian) is added to every frame but the first."""
+    rng = np.random.default_rng(seed + 1000)
+    mover = Mover(texture(h, w, 2.0, rng))
+    shifts = rng.uniform(-max_shift, max_shift, (n, 2))
+    shifts[0] = 0.0
+    frames = np.empty((n, h, w), np.float32)
+    for k in range(n):
+        img = mover.shifted(*shifts[k])
+        if k and noise:
+            img = img + rng.standard_normal(img.shape) * noise
+        frames[k] = img
+    return frames, shifts
