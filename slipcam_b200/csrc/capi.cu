@@ -21,6 +21,7 @@
 
 #include "../../include/slipcam_b200.h"
 #include "corr_fft.cuh"
+#include "corr_big.cuh"
 #include "corr_tc.cuh"
 #include "diff.h"
 #include "sat.cuh"
@@ -47,7 +48,8 @@ void check(cudaError_t e, const char *what)
 #define CK(call) check((call), #call)
 
 // the FFT sizes with a compiled kernel: N = 16 N2 for the radices of dft.cuh
-constexpr int kSizes[] = {16, 32, 48, 64, 80, 96, 128, 144, 160, 192};
+constexpr int kSizes[] = {16, 32, 48, 64, 80, 96, 128, 144, 160, 192, 256};
+constexpr int kBigN = 256;   // the one size whose half spectrum is staged through global memory (corr_big.cuh)
 
 int fft_size(int L)
 {
@@ -136,6 +138,29 @@ int num_sms()
     if (dev < 0 || dev >= 64) return 148;
     if (!g_num_sms[dev]) CK(cudaDeviceGetAttribute(&g_num_sms[dev], cudaDevAttrMultiProcessorCount, dev));
     return g_num_sms[dev];
+}
+
+// the big transform: per-CTA scratch (complex values per CTA), persistent grids of one CTA per SM
+size_t big_scratch_per_cta(int L, int M) { return BigGeo<kBigN>::scratch((L + 1) & ~1, M); }
+
+void prepare_big()
+{
+    static bool done[64] = {};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && done[dev]) return;
+    const int smem = int(BigGeo<kBigN>::smem_bytes);
+    CK(cudaFuncSetAttribute(corr_big_kernel<kBigN, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CK(cudaFuncSetAttribute(spectra_big_kernel<kBigN, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    if (dev >= 0 && dev < 64) done[dev] = true;
+}
+
+void launch_corr_big(const CorrArgs &a, float2 *scratch, cudaStream_t s)
+{
+    prepare_big();
+    const int grid = std::min(a.nwin * a.nf, num_sms());
+    corr_big_kernel<kBigN, kThreads><<<unsigned(grid), kThreads, BigGeo<kBigN>::smem_bytes, s>>>(
+        a, scratch, big_scratch_per_cta(a.L, a.M));
 }
 
 // cuTensorMapEncodeTiled, from the driver through the runtime (no link against libcuda)
@@ -269,6 +294,7 @@ struct b200_handle {
     DevBuf<float> d_norm;
     DevBuf<float2> d_spec, d_tw;
     DevBuf<float4> d_spec_tc;    // the reference spectra in the tensor-core form's order
+    DevBuf<float2> d_big;        // the big transform's per-CTA scratch (N = 256 only)
     DevBuf<uint8_t> d_ref;
     DevBuf<uint32_t> d_sat;      // device-path scratch
     DevBuf<int64_t> d_sat2;
@@ -355,6 +381,8 @@ struct b200_handle {
             if (mi == 2 && dinv != d_dinv.p) fail(B200_EINVAL, "no TMA map for this denominator table");
             const CUtensorMap *dm = d_tmaps.p + mi;
             B200_DISPATCH_TC(N, launch_corr_tc, a, dt, d_status.p, dm, s);
+        } else if (N == kBigN) {
+            launch_corr_big(a, d_big.p, s);
         } else {
             B200_DISPATCH(N, launch_corr, a, s);
         }
@@ -436,7 +464,14 @@ void upload_reference(b200_handle *h, const uint8_t *dframe, int pitch, cudaStre
     a.norm = h->d_norm.p;
     a.spec = h->d_spec.p;
     a.twiddles = h->d_tw.p;
-    B200_DISPATCH(h->N, launch_spectra, a, h->nwin, s);
+    if (h->N == kBigN) {
+        prepare_big();
+        const int grid = std::min(h->nwin, num_sms());
+        spectra_big_kernel<kBigN, kThreads><<<unsigned(grid), kThreads, BigGeo<kBigN>::smem_bytes, s>>>(
+            a, h->nwin, h->d_big.p, big_scratch_per_cta(h->L, h->M));
+    } else {
+        B200_DISPATCH(h->N, launch_spectra, a, h->nwin, s);
+    }
     CK(cudaGetLastError());
     h->launches += 1;
     if (h->tc_ok) {
@@ -509,7 +544,10 @@ int b200_create(const b200_params *p, int device, b200_handle **out)
         const int N = fft_size(L);
         if (!N)
             fail(B200_EINVAL, "the search window (window + 2 search = " + std::to_string(L)
-                                  + ") is larger than the b200 backend's largest transform, 192");
+                                  + ") is larger than the b200 backend's largest transform, 256");
+        if (N == kBigN && !BigGeo<kBigN>::fits_M(2 * p->search + 1))
+            fail(B200_EINVAL, "with a search window of " + std::to_string(L)
+                                  + " pixels the b200 backend holds searches up to 64 pixels");
         h = new b200_handle;
         h->height = p->height;
         h->width = p->width;
@@ -555,6 +593,7 @@ int b200_create(const b200_params *p, int device, b200_handle **out)
             h->d_spec_tc.alloc(size_t(h->nwin) * (N / 2) * tc_kp(N));
             CK(cudaMemcpy(h->d_dtab.p, dt.data(), dt.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
         }
+        if (N == kBigN) h->d_big.alloc(size_t(num_sms()) * big_scratch_per_cta(L, h->M));
         const size_t G = size_t(h->group), P = G * h->nwin;
         h->d_sat.alloc(G * h->sat_size());
         h->d_sat2.alloc(G * h->sat_size());
@@ -866,7 +905,10 @@ int b200_correlate_device_noalloc(b200_handle *h, const uint8_t *frames, int n, 
             a.snr = snr + q0;
             a.cov = cov + 3 * q0;
             a.surface = nullptr;
-            B200_DISPATCH(h->N, launch_corr, a, s);
+            if (h->N == kBigN)
+                launch_corr_big(a, h->d_big.p, s);
+            else
+                B200_DISPATCH(h->N, launch_corr, a, s);
             CK(cudaGetLastError());
             h->launches += 4;
         }

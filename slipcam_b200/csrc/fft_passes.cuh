@@ -131,17 +131,20 @@ B200_HD void row_forward(const Ex &ex, float2 *S, int P, const float2 *TW, int o
     });
 }
 
-// The column pass over the NH columns of the half spectrum (rows [0, Lr) nonzero).
+// The column pass over `ncols` columns of the half spectrum (rows [0, Lr) nonzero; by default all
+// NH of them, `stride` complex values apart per row, NHP by default; a subset of the columns
+// starting at k0 is passed as S, spec or out moved by k0 columns).
 // CORR false: the forward spectra are written to out[k * N + k2 * 16 + k1] (frequency
 //   k1 + 16 k2 of column k).
 // CORR true: the forward spectra are multiplied by conj(spec[k * N + k2 * 16 + k1]) (the same
 //   order), transformed back, and rows [0, M) of each column stored in S.
 template <int N, bool CORR, class Ex>
 B200_HD void col_pass(const Ex &ex, float2 *S, int Lr, int M, const float2 *TW, const float2 *TWI,
-                      const float2 *spec, float2 *out)
+                      const float2 *spec, float2 *out, int ncols = Geo<N>::NH, int stride = Geo<N>::NHP)
 {
     using G = Geo<N>;
-    constexpr int N2 = G::N2, NHP = G::NHP, NH = G::NH;
+    constexpr int N2 = G::N2;
+    const int NHP = stride, NH = ncols;
     struct St {
         float2 y[16];
         float2 z[N2];

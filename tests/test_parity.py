@@ -22,7 +22,7 @@ from slipcam_b200 import framecor, synth
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip('torch')
 
-SUPPORTED = [n for n in cases.NAMES if n != 'big']   # window 128 + search 64: L = 256, not yet
+SUPPORTED = list(cases.NAMES)   # 'big' (window 128 + search 64, L = 256) runs the staged big transform
 NEAR_TIE = 1e-5
 # the share of integer peaks allowed to differ, each one a verified near-tie; 'mixed' has periodic
 # stripes (8 px) whose surfaces have exactly equal maxima, decided by rounding alone
@@ -257,3 +257,27 @@ def test_tc_form_limits():
         cor.set_form('tc')
     with pytest.raises(ValueError):
         cor.set_form('bf16')
+
+
+def test_big_transform_surfaces_match_fp64_oracle():
+    """L = 256 (window 128, search 64): the staged N = 256 transform's surfaces against the FP64
+    direct oracle on every pair of the golden case."""
+    c = cases.case('big')
+    cor = framecor.Correlator(c['height'], c['width'], c['down'], c['across'], window=128, search=64,
+                              stat_size=c['stat_size'], backend='b200')
+    cor.set_reference(c['reference'])
+    assert cor.info()[2] == 256
+    out = cor.correlate(torch.as_tensor(c['frames']).cuda(), surfaces=True)
+    o = oracle.correlate(c['height'], c['width'], c['down'], c['across'], c['reference'], c['frames'], None,
+                         window=128, search=64, stat_size=c['stat_size'], mode='f64', surfaces=True)
+    assert np.abs(out['surface'].cpu().numpy() - o['surface']).max() < 2e-5
+    d = np.abs(out['offsets'].cpu().numpy() - o['offsets64'])
+    assert np.array_equal(np.isnan(d), np.isnan(o['offsets64']))
+    assert np.nanmax(d) < 1e-3
+
+
+def test_search_beyond_big_transform_rejected():
+    """Past the staged transform's limit (search 64 at L up to 256) a clear ValueError."""
+    down, across = framecor.window_grid(512, 512, 32, 100, 64)   # L = 232, M = 201
+    with pytest.raises(ValueError, match='searches up to 64'):
+        framecor.Correlator(512, 512, down, across, window=32, search=100, backend='b200')
