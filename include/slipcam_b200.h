@@ -125,6 +125,41 @@ B200_API int b200_correlate_device_noalloc(b200_handle *h, const uint8_t *frames
                                            const int32_t *gross, int gross_mode, float *offset,
                                            float *peak, float *snr, float *cov, void *stream);
 
+/* ---- Several window grids of one video in one persistent launch (window sizes, search ranges
+ * and grids may all differ). No counterpart in the reference, which correlates one grid per
+ * Correlator (cxx/framecor.h:46-56); a group of handles created by b200_create (same frame size
+ * and device, each with its reference set) is correlated together: the frames' summed-area
+ * tables once, one variance-denominator table per window size, then one persistent launch of the
+ * FP32 FFT correlation over every grid's (window, frame) pairs, scheduled dynamically (the
+ * costliest grid first by default). The step is captured in a CUDA graph on the group's own
+ * stream and replayed while the caller's pointers and sizes stay the same.
+ * The handles stay owned by the caller and must outlive the group. Up to 4 grids. */
+typedef struct b200_group b200_group;
+B200_API int b200_group_create(b200_handle *const *grids, int count, b200_group **out);
+B200_API int b200_group_destroy(b200_group *g);
+B200_API const char *b200_group_last_error(const b200_group *g);
+
+/* n frames (device memory, rows `pitch` bytes apart) through every grid: per grid i, gross[i] /
+ * gross_mode[i] as for b200_correlate_device (gross may be NULL: no gross for any grid) and its
+ * outputs offset[i], peak[i], snr[i], cov[i] (device memory). Stream-ordered on `stream`. */
+B200_API int b200_group_correlate_device(b200_group *g, const uint8_t *frames, int n, int pitch,
+                                         const int32_t *const *gross, const int *gross_mode,
+                                         float *const *offset, float *const *peak, float *const *snr,
+                                         float *const *cov, void *stream);
+
+/* The autotuner: times the persistent launch on these frames for every candidate of threads per
+ * CTA (256, 512), (window, frame) pairs per work item (1, 2, 4, 8) and grid order (costliest
+ * first or as given), keeps the fastest and returns its time (ms per launch). Synchronous;
+ * allocates its own temporary outputs. */
+B200_API int b200_group_tune(b200_group *g, const uint8_t *frames, int n, int pitch,
+                             const int32_t *const *gross, const int *gross_mode, void *stream,
+                             double *best_ms);
+
+/* The launch configuration (threads per CTA, pairs per work item, costliest grid first, CUDA
+ * graph replay), read or set. */
+B200_API int b200_group_config(const b200_group *g, int *threads, int *chunk, int *costly_first, int *use_graph);
+B200_API int b200_group_set_config(b200_group *g, int threads, int chunk, int costly_first, int use_graph);
+
 /* ---- The differentiable path: float frames, a continuous shift per pair, and the adjoints.
  * No counterpart in the reference (its backends take uint8 frames and give no derivatives); the
  * math follows the same correlation (cxx/cpu.cpp:115-160, cxx/surface.h:30-146) and is stated in

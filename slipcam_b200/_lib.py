@@ -34,6 +34,16 @@ SIGNATURES = {
     'b200_correlate_device': (_i, [_vp, _u8p, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp]),
     'b200_correlate_device_surfaces': (_i, [_vp, _u8p, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
     'b200_correlate_device_noalloc': (_i, [_vp, _u8p, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp]),
+    'b200_group_create': (_i, [ctypes.POINTER(_vp), _i, ctypes.POINTER(_vp)]),
+    'b200_group_destroy': (_i, [_vp]),
+    'b200_group_last_error': (ctypes.c_char_p, [_vp]),
+    'b200_group_correlate_device': (_i, [_vp, _u8p, _i, _i, ctypes.POINTER(_vp), ctypes.POINTER(_i),
+                                         ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp),
+                                         ctypes.POINTER(_vp), _vp]),
+    'b200_group_tune': (_i, [_vp, _u8p, _i, _i, ctypes.POINTER(_vp), ctypes.POINTER(_i), _vp,
+                             ctypes.POINTER(ctypes.c_double)]),
+    'b200_group_config': (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    'b200_group_set_config': (_i, [_vp, _i, _i, _i, _i]),
     'b200_set_reference_f32_device': (_i, [_vp, _vp, _i, _vp]),
     'b200_diff_forward': (_i, [_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     'b200_diff_backward': (_i, [_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
@@ -79,11 +89,12 @@ def loaded():
         return False
 
 
-def raise_for(rc, handle=None):
+def raise_for(rc, handle=None, group=False):
     """The reference's exception for a status code (ValueError / RuntimeError)."""
     if rc == OK:
         return
-    msg = lib().b200_last_error(handle).decode() or f'framecor: error {rc}'
+    err = lib().b200_group_last_error if group else lib().b200_last_error
+    msg = err(handle).decode() or f'framecor: error {rc}'
     if rc == EINVAL:
         raise ValueError(msg)
     raise RuntimeError(msg)

@@ -24,6 +24,7 @@
 #include "corr_big.cuh"
 #include "corr_tc.cuh"
 #include "diff.h"
+#include "multi.h"
 #include "sat.cuh"
 #include "tc_selftest.cuh"
 
@@ -445,6 +446,9 @@ int guarded(b200_handle *h, F &&f)
     } catch (const std::bad_alloc &) {
         h->err = "framecor: out of host memory";
         return B200_ERUNTIME;
+    } catch (const std::invalid_argument &e) {
+        h->err = std::string("framecor: ") + e.what();
+        return B200_EINVAL;
     } catch (const std::exception &e) {
         h->err = std::string("framecor: ") + e.what();
         return B200_ERUNTIME;
@@ -1063,5 +1067,387 @@ int b200_has_device(void)
 }
 
 const char *b200_version(void) { return "0.1.0"; }
+
+}   // extern "C"
+
+// ---- groups of grids in one persistent launch (multi.h, multi.cu)
+
+struct b200_group {
+    std::vector<b200_handle *> grids;
+    int height = 0, width = 0, device = 0;
+    std::string err;
+    cudaStream_t stream = nullptr;       // the group's own stream: graph capture and replay
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    int cap = 0;                         // frames the per-call tables hold
+    DevBuf<uint32_t> sat;
+    DevBuf<int64_t> sat2;
+    std::vector<int> wsizes;             // the distinct window sizes, one denominator table each
+    std::vector<DevBuf<float>> dinv;
+    DevBuf<int> counter;
+    DevBuf<MultiArgs> args;
+    DevBuf<float2> big;                  // the N = 256 grid's per-CTA scratch
+    size_t big_per_cta = 0;
+    int nt = 256, chunk = 1;             // the launch configuration (b200_group_tune)
+    bool costly_first = true, use_graph = true;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uintptr_t> key;          // what the captured step was made for
+    uint64_t launches = 0;
+
+    ~b200_group()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (ev_in) cudaEventDestroy(ev_in);
+        if (ev_out) cudaEventDestroy(ev_out);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    int64_t sat_size() const { return int64_t(height + 1) * (width + 1); }
+    int dpitch() const { return (width + 3) & ~3; }
+    int64_t dinv_size() const { return int64_t(height) * dpitch(); }
+
+    size_t smem() const
+    {
+        size_t m = 0;
+        for (const b200_handle *h : grids) m = std::max(m, multi_smem(h->N));
+        return m;
+    }
+
+    int grid_ctas() const { return num_sms() * multi_occupancy(nt, smem()); }
+
+    // the per-call tables for n frames and the big scratch for the current grid size
+    void reserve(int n)
+    {
+        const size_t need_big = size_t(grid_ctas()) * big_per_cta;
+        if (n <= cap && big.n >= need_big) return;
+        CK(cudaStreamSynchronize(stream));   // nothing in flight may still read them
+        if (n > cap) {
+            sat.alloc(size_t(n) * sat_size());
+            sat2.alloc(size_t(n) * sat_size());
+            for (DevBuf<float> &d : dinv) d.alloc(size_t(n) * dinv_size());
+            cap = n;
+        }
+        if (big.n < need_big) big.alloc(need_big);
+        key.clear();
+    }
+
+    // the arguments of one launch over n frames
+    MultiArgs make_args(const uint8_t *frames, int n, int pitch, const int32_t *const *gross, const int *mode,
+                        float *const *offset, float *const *peak, float *const *snr, float *const *cov) const
+    {
+        MultiArgs m{};
+        m.ngrids = int(grids.size());
+        for (int i = 0; i < m.ngrids; ++i) {
+            const b200_handle *h = grids[size_t(i)];
+            CorrArgs &a = m.g[i].a;
+            a.frames = frames;
+            a.fstride = int64_t(pitch) * height;
+            a.pitch = pitch;
+            a.sat = sat.p;
+            a.sat_fstride = sat_size();
+            const size_t wi = size_t(std::find(wsizes.begin(), wsizes.end(), h->W) - wsizes.begin());
+            a.dinv = dinv[wi].p;
+            a.dinv_fstride = dinv_size();
+            a.dpitch = dpitch();
+            a.h = height;
+            a.w = width;
+            a.W = h->W;
+            a.R = h->R;
+            a.L = h->L;
+            a.M = h->M;
+            a.nx = h->nx;
+            a.nwin = h->nwin;
+            a.nf = n;
+            a.stat = h->stat;
+            a.down = h->d_down.p;
+            a.across = h->d_across.p;
+            a.norm = h->d_norm.p;
+            a.spec = h->d_spec.p;
+            a.twiddles = h->d_tw.p;
+            a.gross = gross ? gross[i] : nullptr;
+            a.gross_mode = gross && gross[i] ? mode[i] : 0;
+            a.offset = offset[i];
+            a.peak = peak[i];
+            a.snr = snr[i];
+            a.cov = cov[i];
+            m.g[i].N = h->N;
+            m.g[i].chunk = chunk;
+            m.g[i].items = int((int64_t(h->nwin) * n + chunk - 1) / chunk);
+            m.total_items += m.g[i].items;
+            m.order[i] = i;
+        }
+        if (costly_first) {   // by the work of one pair, N^2 log N
+            auto cost = [&](int i) { const double N = grids[size_t(i)]->N; return N * N * std::log2(N); };
+            std::stable_sort(m.order, m.order + m.ngrids, [&](int x, int y) { return cost(x) > cost(y); });
+        }
+        m.counter = counter.p;
+        m.big_scratch = big.p;
+        m.big_per_cta = big_per_cta;
+        return m;
+    }
+
+    // the step on the group's stream: tables, denominators, the persistent launch
+    void step(const uint8_t *frames, int n, int pitch)
+    {
+        launch_sat(frames, int64_t(pitch) * height, pitch, n, height, width, sat.p, sat2.p, stream);
+        for (size_t wi = 0; wi < wsizes.size(); ++wi) {
+            const int W = wsizes[wi];
+            dinv_kernel<<<dim3(unsigned((width - W + 1 + 127) / 128), unsigned(height - W + 1), unsigned(n)), 128, 0, stream>>>(
+                sat.p, sat2.p, sat_size(), height, width, W, dinv[wi].p, dinv_size(), dpitch());
+        }
+        CK(cudaMemsetAsync(counter.p, 0, sizeof(int), stream));
+        launch_corr_multi(args.p, nt, smem(), grid_ctas(), stream);
+        CK(cudaGetLastError());
+    }
+};
+
+namespace {
+
+template <class F>
+int guarded_group(b200_group *g, F &&f)
+{
+    if (!g) return B200_EINVAL;
+    try {
+        f();
+        g->err.clear();
+        return B200_OK;
+    } catch (const Failure &e) {
+        g->err = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        g->err = "framecor: out of host memory";
+        return B200_ERUNTIME;
+    } catch (const std::invalid_argument &e) {
+        g->err = std::string("framecor: ") + e.what();
+        return B200_EINVAL;
+    } catch (const std::exception &e) {
+        g->err = std::string("framecor: ") + e.what();
+        return B200_ERUNTIME;
+    }
+}
+
+void check_group_call(const b200_group *g, const uint8_t *frames, int n, int pitch, const int32_t *const *gross,
+                      const int *mode)
+{
+    if (n < 0) fail(B200_EINVAL, "the number of frames must not be negative");
+    if (n && (!frames || pitch < g->width)) fail(B200_EINVAL, "no frames, or their pitch is below their width");
+    for (size_t i = 0; i < g->grids.size(); ++i) {
+        if (!g->grids[i]->ready) fail(B200_ERUNTIME, "set_reference first (grid " + std::to_string(i) + ")");
+        if (gross && gross[i] && (!mode || mode[i] < B200_GROSS_FRAME || mode[i] > B200_GROSS_WINDOW))
+            fail(B200_EINVAL, "gross must be frames x 2 or frames x down x across x 2");
+    }
+}
+
+}   // namespace
+
+extern "C" {
+
+int b200_group_create(b200_handle *const *grids, int count, b200_group **out)
+{
+    if (out) *out = nullptr;
+    b200_group *g = nullptr;
+    try {
+        if (!out || !grids) fail(B200_EINVAL, "no grids or no output");
+        if (count < 1 || count > kMaxGrids) fail(B200_EINVAL, "a group holds 1 to 4 grids");
+        g = new b200_group;
+        for (int i = 0; i < count; ++i) {
+            b200_handle *h = grids[i];
+            if (!h) fail(B200_EINVAL, "a null grid");
+            if (i && (h->height != g->height || h->width != g->width || h->device != g->device))
+                fail(B200_EINVAL, "the grids of a group must share the frame size and the device");
+            if (!multi_supports(h->N)) fail(B200_EINVAL, "no multi-grid kernel for the FFT size " + std::to_string(h->N));
+            g->height = h->height;
+            g->width = h->width;
+            g->device = h->device;
+            g->grids.push_back(h);
+            if (std::find(g->wsizes.begin(), g->wsizes.end(), h->W) == g->wsizes.end()) g->wsizes.push_back(h->W);
+            if (h->N == kBigN) g->big_per_cta = std::max(g->big_per_cta, big_scratch_per_cta(h->L, h->M));
+        }
+        CK(cudaSetDevice(g->device));
+        CK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&g->ev_in, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&g->ev_out, cudaEventDisableTiming));
+        g->dinv.resize(g->wsizes.size());
+        g->counter.alloc(1);
+        g->args.alloc(1);
+        prepare_multi();
+        if (g->big_per_cta) prepare_big();
+        *out = g;
+        return B200_OK;
+    } catch (const Failure &e) {
+        g_create_error = e.msg;
+        delete g;
+        return e.code;
+    } catch (const std::exception &e) {
+        g_create_error = std::string("framecor: ") + e.what();
+        delete g;
+        return B200_ERUNTIME;
+    }
+}
+
+int b200_group_destroy(b200_group *g)
+{
+    if (!g) return B200_EINVAL;
+    cudaSetDevice(g->device);
+    cudaStreamSynchronize(g->stream);
+    delete g;
+    return B200_OK;
+}
+
+const char *b200_group_last_error(const b200_group *g) { return g ? g->err.c_str() : g_create_error.c_str(); }
+
+int b200_group_correlate_device(b200_group *g, const uint8_t *frames, int n, int pitch, const int32_t *const *gross,
+                                const int *gross_mode, float *const *offset, float *const *peak, float *const *snr,
+                                float *const *cov, void *stream)
+{
+    return guarded_group(g, [&] {
+        check_group_call(g, frames, n, pitch, gross, gross_mode);
+        if (n == 0) return;
+        if (!offset || !peak || !snr || !cov) fail(B200_EINVAL, "null outputs");
+        for (size_t i = 0; i < g->grids.size(); ++i)
+            if (!offset[i] || !peak[i] || !snr[i] || !cov[i]) fail(B200_EINVAL, "null outputs");
+        CK(cudaSetDevice(g->device));
+        g->reserve(n);
+        cudaStream_t user = static_cast<cudaStream_t>(stream);
+        // what the step is made for: a captured graph stays valid while all of it is unchanged
+        std::vector<uintptr_t> key = {uintptr_t(frames), uintptr_t(n), uintptr_t(pitch), uintptr_t(g->nt),
+                                      uintptr_t(g->chunk), uintptr_t(g->costly_first)};
+        for (size_t i = 0; i < g->grids.size(); ++i) {
+            key.push_back(gross ? uintptr_t(gross[i]) : 0);
+            key.push_back(gross && gross[i] ? uintptr_t(gross_mode[i]) : 0);
+            for (float *const *o : {offset, peak, snr, cov}) key.push_back(uintptr_t(o[i]));
+        }
+        CK(cudaEventRecord(g->ev_in, user));
+        CK(cudaStreamWaitEvent(g->stream, g->ev_in, 0));
+        if (key != g->key) {
+            CK(cudaStreamSynchronize(g->stream));   // a step in flight may still read the arguments
+            const MultiArgs m = g->make_args(frames, n, pitch, gross, gross_mode, offset, peak, snr, cov);
+            CK(cudaMemcpy(g->args.p, &m, sizeof(MultiArgs), cudaMemcpyHostToDevice));
+            if (g->use_graph) {
+                cudaGraph_t graph = nullptr;
+                CK(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+                try {
+                    g->step(frames, n, pitch);
+                } catch (...) {
+                    cudaStreamEndCapture(g->stream, &graph);
+                    if (graph) cudaGraphDestroy(graph);
+                    throw;
+                }
+                CK(cudaStreamEndCapture(g->stream, &graph));
+                cudaGraphExecUpdateResultInfo info{};
+                if (!g->exec || cudaGraphExecUpdate(g->exec, graph, &info) != cudaSuccess) {
+                    cudaGetLastError();
+                    if (g->exec) cudaGraphExecDestroy(g->exec);
+                    g->exec = nullptr;
+                    const cudaError_t e = cudaGraphInstantiate(&g->exec, graph, 0);
+                    cudaGraphDestroy(graph);
+                    CK(e);
+                } else {
+                    cudaGraphDestroy(graph);
+                }
+            }
+            g->key = key;
+        }
+        if (g->use_graph)
+            CK(cudaGraphLaunch(g->exec, g->stream));
+        else
+            g->step(frames, n, pitch);
+        CK(cudaEventRecord(g->ev_out, g->stream));
+        CK(cudaStreamWaitEvent(user, g->ev_out, 0));
+        g->launches += 3 + g->wsizes.size();
+    });
+}
+
+int b200_group_tune(b200_group *g, const uint8_t *frames, int n, int pitch, const int32_t *const *gross,
+                    const int *gross_mode, void *stream, double *best_ms)
+{
+    return guarded_group(g, [&] {
+        check_group_call(g, frames, n, pitch, gross, gross_mode);
+        if (n == 0) fail(B200_EINVAL, "the autotuner needs frames");
+        CK(cudaSetDevice(g->device));
+        CK(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+        const size_t ng = g->grids.size();
+        std::vector<DevBuf<float>> outs(ng);
+        std::vector<float *> off(ng), pk(ng), sn(ng), cv(ng);
+        for (size_t i = 0; i < ng; ++i) {
+            const size_t P = size_t(n) * g->grids[i]->nwin;
+            outs[i].alloc(7 * P);
+            off[i] = outs[i].p;
+            pk[i] = off[i] + 2 * P;
+            sn[i] = pk[i] + P;
+            cv[i] = sn[i] + P;
+        }
+        cudaEvent_t t0, t1;
+        CK(cudaEventCreate(&t0));
+        CK(cudaEventCreate(&t1));
+        double best = 1e30;
+        int bnt = g->nt, bchunk = g->chunk;
+        bool bfirst = g->costly_first;
+        try {
+            for (int nt : {256, 512})
+                for (int chunk : {1, 2, 4, 8})
+                    for (bool first : {true, false}) {
+                        g->nt = nt;
+                        g->chunk = chunk;
+                        g->costly_first = first;
+                        g->reserve(n);
+                        const MultiArgs m = g->make_args(frames, n, pitch, gross, gross_mode, off.data(), pk.data(),
+                                                         sn.data(), cv.data());
+                        CK(cudaMemcpy(g->args.p, &m, sizeof(MultiArgs), cudaMemcpyHostToDevice));
+                        g->step(frames, n, pitch);   // tables and a warm-up
+                        float ms = 0.0f, total = 0.0f;
+                        for (int r = 0; r < 3; ++r) {
+                            CK(cudaMemsetAsync(g->counter.p, 0, sizeof(int), g->stream));
+                            CK(cudaEventRecord(t0, g->stream));
+                            launch_corr_multi(g->args.p, g->nt, g->smem(), g->grid_ctas(), g->stream);
+                            CK(cudaEventRecord(t1, g->stream));
+                            CK(cudaEventSynchronize(t1));
+                            CK(cudaEventElapsedTime(&ms, t0, t1));
+                            total += ms;
+                        }
+                        if (total / 3 < best) {
+                            best = total / 3;
+                            bnt = nt;
+                            bchunk = chunk;
+                            bfirst = first;
+                        }
+                    }
+        } catch (...) {
+            cudaEventDestroy(t0);
+            cudaEventDestroy(t1);
+            throw;
+        }
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        CK(cudaStreamSynchronize(g->stream));
+        g->nt = bnt;
+        g->chunk = bchunk;
+        g->costly_first = bfirst;
+        g->key.clear();
+        if (best_ms) *best_ms = best;
+    });
+}
+
+int b200_group_config(const b200_group *g, int *threads, int *chunk, int *costly_first, int *use_graph)
+{
+    if (!g) return B200_EINVAL;
+    if (threads) *threads = g->nt;
+    if (chunk) *chunk = g->chunk;
+    if (costly_first) *costly_first = g->costly_first;
+    if (use_graph) *use_graph = g->use_graph;
+    return B200_OK;
+}
+
+int b200_group_set_config(b200_group *g, int threads, int chunk, int costly_first, int use_graph)
+{
+    return guarded_group(g, [&] {
+        if ((threads != 256 && threads != 512) || chunk < 1 || chunk > 64)
+            fail(B200_EINVAL, "threads must be 256 or 512 and chunk 1 to 64");
+        g->nt = threads;
+        g->chunk = chunk;
+        g->costly_first = costly_first != 0;
+        g->use_graph = use_graph != 0;
+        g->key.clear();
+    });
+}
 
 }   // extern "C"

@@ -149,64 +149,73 @@ __global__ void __launch_bounds__(NT, 1) spectra_big_kernel(SpectraArgs a, int n
     for (int k = blockIdx.x; k < nwin; k += gridDim.x) big_window<N, NT>(a, k, W, TW, TWI, gs);
 }
 
-// the correlation of the big transform: persistent CTAs over the pairs of the group
+// one (window, frame) pair p of the big transform in the work area W (BigGeo<N>::smem_bytes,
+// twiddles included) with this CTA's scratch gs. Every thread of the block calls it and it ends
+// with a barrier (the next pair may reuse W at once).
 template <int N, int NT>
-__global__ void __launch_bounds__(NT, 1) corr_big_kernel(CorrArgs a, float2 *scratch, size_t per_cta)
+__device__ void corr_big_pair(const CorrArgs &a, int p, float2 *W, float2 *gs)
 {
     using B = BigGeo<N>;
-    extern __shared__ float4 smem_raw[];
-    float2 *W = reinterpret_cast<float2 *>(smem_raw);
     float2 *TW = W + B::work_bytes / sizeof(float2), *TWI = TW + N;
     float *Sr = reinterpret_cast<float *>(W);
     const int L = a.L, M = a.M, R = a.R;
     const int Lr = (L + 1) & ~1;
-    float2 *gs = scratch + size_t(blockIdx.x) * per_cta;
     float2 *gm = gs + size_t(Lr) * B::NH;
+    const int k = p / a.nf, f = p % a.nf;
+    const int64_t q = int64_t(f) * a.nwin + k;
+    int gy = 0, gx = 0;
+    if (a.gross_mode == 1) {
+        gy = a.gross[2 * f];
+        gx = a.gross[2 * f + 1];
+    } else if (a.gross_mode == 2) {
+        gy = a.gross[2 * q];
+        gx = a.gross[2 * q + 1];
+    }
+    const int sy = a.down[k / a.nx] + gy - R, sx = a.across[k % a.nx] + gx - R;
+    const float norm = a.norm[k];
+    if (!(norm > 0) || sy < 0 || sx < 0 || sy + L > a.h || sx + L > a.w) {   // cxx/surface.h:39-45
+        if (threadIdx.x == 0) invalid_outputs(q, a.offset, a.peak, a.snr, a.cov);
+        if (a.surface)
+            for (int i = threadIdx.x; i < M * M; i += NT) a.surface[q * M * M + i] = 0.0f;
+        return;
+    }
     for (int i = threadIdx.x; i < 2 * N; i += NT) TW[i] = a.twiddles[i];
+    // the chip minus its mean, float(box sum) / (L L) as cxx/cpu.cpp:132
+    const uint32_t *sat = a.sat + size_t(f) * a.sat_fstride;
+    const size_t ss = size_t(a.w) + 1;
+    const uint32_t box = sat[(sy + L) * ss + sx + L] - sat[sy * ss + sx + L] - sat[(sy + L) * ss + sx] + sat[sy * ss + sx];
+    const float mean = float(box) / (float(L) * float(L));
+    const uint8_t *chip = a.frames + f * a.fstride + int64_t(sy) * a.pitch + sx;
+    big_rows<N, NT>(W, TW, Lr, L, gs, [&](int i, int j) { return float(__ldg(chip + int64_t(i) * a.pitch + j)) - mean; });
+    big_cols<N, NT, true>(W, TW, TWI, Lr, M, gs, a.spec + size_t(k) * B::NH * N, nullptr, gm);
+    // rows [0, M) of the column-inverted spectrum, whole again, then the inverse row pass
+    for (int idx = threadIdx.x; idx < M * B::NH; idx += NT) {
+        const int u = idx / B::NH, c = idx % B::NH;
+        W[size_t(u) * B::NHP + c] = gm[size_t(u) * B::NH + c];
+    }
     __syncthreads();
+    const float inv = 1.0f / (float(N) * float(N) * norm);
+    const float *dinv = a.dinv + size_t(f) * a.dinv_fstride + size_t(sy) * a.dpitch + sx;
+    const int dw = a.dpitch;
+    const DevExec ex{int(threadIdx.x >> 5), NT / 32};
+    row_inverse<N>(ex, W, M, TWI, [&](int u, int c, float x) { return x * inv * __ldg(dinv + size_t(u) * dw + c); });
+    __syncthreads();
+    if (a.surface)
+        for (int i = threadIdx.x; i < M * M; i += NT) a.surface[q * M * M + i] = Sr[size_t(i / M) * B::RP + i % M];
+    surface_peak<NT>(Sr, B::RP, M, R, a.stat, gy, gx, a.W * a.W, q, a.offset, a.peak, a.snr, a.cov, nullptr);
+    __syncthreads();
+}
+
+// the correlation of the big transform: persistent CTAs over the pairs of the group, scratch per CTA
+template <int N, int NT>
+__global__ void __launch_bounds__(NT, 1) corr_big_kernel(CorrArgs a, float2 *scratch, size_t per_cta)
+{
+    extern __shared__ float4 smem_raw[];
+    float2 *W = reinterpret_cast<float2 *>(smem_raw);
+    float2 *gs = scratch + size_t(blockIdx.x) * per_cta;
     const int npairs = a.nwin * a.nf;
     for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
-        const int k = p / a.nf, f = p % a.nf;
-        const int64_t q = int64_t(f) * a.nwin + k;
-        int gy = 0, gx = 0;
-        if (a.gross_mode == 1) {
-            gy = a.gross[2 * f];
-            gx = a.gross[2 * f + 1];
-        } else if (a.gross_mode == 2) {
-            gy = a.gross[2 * q];
-            gx = a.gross[2 * q + 1];
-        }
-        const int sy = a.down[k / a.nx] + gy - R, sx = a.across[k % a.nx] + gx - R;
-        const float norm = a.norm[k];
-        if (!(norm > 0) || sy < 0 || sx < 0 || sy + L > a.h || sx + L > a.w) {   // cxx/surface.h:39-45
-            if (threadIdx.x == 0) invalid_outputs(q, a.offset, a.peak, a.snr, a.cov);
-            if (a.surface)
-                for (int i = threadIdx.x; i < M * M; i += NT) a.surface[q * M * M + i] = 0.0f;
-            continue;
-        }
-        // the chip minus its mean, float(box sum) / (L L) as cxx/cpu.cpp:132
-        const uint32_t *sat = a.sat + size_t(f) * a.sat_fstride;
-        const size_t ss = size_t(a.w) + 1;
-        const uint32_t box = sat[(sy + L) * ss + sx + L] - sat[sy * ss + sx + L] - sat[(sy + L) * ss + sx] + sat[sy * ss + sx];
-        const float mean = float(box) / (float(L) * float(L));
-        const uint8_t *chip = a.frames + f * a.fstride + int64_t(sy) * a.pitch + sx;
-        big_rows<N, NT>(W, TW, Lr, L, gs, [&](int i, int j) { return float(__ldg(chip + int64_t(i) * a.pitch + j)) - mean; });
-        big_cols<N, NT, true>(W, TW, TWI, Lr, M, gs, a.spec + size_t(k) * B::NH * N, nullptr, gm);
-        // rows [0, M) of the column-inverted spectrum, whole again, then the inverse row pass
-        for (int idx = threadIdx.x; idx < M * B::NH; idx += NT) {
-            const int u = idx / B::NH, c = idx % B::NH;
-            W[size_t(u) * B::NHP + c] = gm[size_t(u) * B::NH + c];
-        }
-        __syncthreads();
-        const float inv = 1.0f / (float(N) * float(N) * norm);
-        const float *dinv = a.dinv + size_t(f) * a.dinv_fstride + size_t(sy) * a.dpitch + sx;
-        const int dw = a.dpitch;
-        const DevExec ex{int(threadIdx.x >> 5), NT / 32};
-        row_inverse<N>(ex, W, M, TWI, [&](int u, int c, float x) { return x * inv * __ldg(dinv + size_t(u) * dw + c); });
-        __syncthreads();
-        if (a.surface)
-            for (int i = threadIdx.x; i < M * M; i += NT) a.surface[q * M * M + i] = Sr[size_t(i / M) * B::RP + i % M];
-        surface_peak<NT>(Sr, B::RP, M, R, a.stat, gy, gx, a.W * a.W, q, a.offset, a.peak, a.snr, a.cov, nullptr);
+        corr_big_pair<N, NT>(a, p, W, gs);
         __syncthreads();
     }
 }

@@ -231,17 +231,15 @@ __global__ void __launch_bounds__(NT) spectra_kernel(SpectraArgs a)
     col_pass<N, false>(ex, S, Wr, 0, TW, TWI, nullptr, a.spec + size_t(k) * G::NH * N);
 }
 
-// the correlation of one (window, frame) pair per CTA; blockIdx.x = window * nf + frame, so the
-// CTAs of one window (one reference spectrum) run together and share it through L2
+// one (window k, frame f) pair: the correlation, normalized, and its outputs, in the shared-memory
+// tile S (Geo<N>::smem_bytes). Every thread of the block calls it; warp 0 may still be writing the
+// pair's outputs when the others return, so a caller that reuses S syncs first.
 template <int N, int NT>
-__global__ void __launch_bounds__(NT, (N <= 160 ? 2 : 1)) corr_kernel(CorrArgs a)
+__device__ __forceinline__ void corr_pair(const CorrArgs &a, int k, int f, float2 *S)
 {
     using G = Geo<N>;
-    extern __shared__ float4 smem_raw[];
-    float2 *S = reinterpret_cast<float2 *>(smem_raw);
     float2 *TW = S + size_t(N) * G::NHP, *TWI = TW + N;
     float *Sr = reinterpret_cast<float *>(S);
-    const int k = blockIdx.x / a.nf, f = blockIdx.x % a.nf;
     const int64_t q = int64_t(f) * a.nwin + k;
     const int warp = threadIdx.x >> 5;
 
@@ -321,6 +319,15 @@ __global__ void __launch_bounds__(NT, (N <= 160 ? 2 : 1)) corr_kernel(CorrArgs a
         for (int i = threadIdx.x; i < M * M; i += NT) a.surface[q * M * M + i] = Sr[size_t(i / M) * G::RP + i % M];
 
     surface_peak<NT>(Sr, G::RP, M, R, a.stat, gy, gx, a.W * a.W, q, a.offset, a.peak, a.snr, a.cov, nullptr);
+}
+
+// the correlation of one (window, frame) pair per CTA; blockIdx.x = window * nf + frame, so the
+// CTAs of one window (one reference spectrum) run together and share it through L2
+template <int N, int NT>
+__global__ void __launch_bounds__(NT, (N <= 160 ? 2 : 1)) corr_kernel(CorrArgs a)
+{
+    extern __shared__ float4 smem_raw[];
+    corr_pair<N, NT>(a, blockIdx.x / a.nf, blockIdx.x % a.nf, reinterpret_cast<float2 *>(smem_raw));
 }
 
 #endif   // __CUDACC__

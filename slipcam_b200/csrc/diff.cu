@@ -13,7 +13,7 @@ constexpr int kNT = 256;
 
 void ck(cudaError_t e, const char *what)
 {
-    if (e != cudaSuccess) throw std::runtime_error(std::string("framecor: ") + what + ": " + cudaGetErrorString(e));
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
 // the dynamic shared memory limits, once per device and kernel instance
@@ -59,14 +59,14 @@ void adjoint(const DiffArgs &a, unsigned pairs, cudaStream_t s)
     case 144: F<144>(__VA_ARGS__); break;                                                          \
     case 160: F<160>(__VA_ARGS__); break;                                                          \
     case 192: F<192>(__VA_ARGS__); break;                                                          \
-    default: throw std::invalid_argument("framecor: no differentiable kernel for the FFT size " + std::to_string(N_)); \
+    default: throw std::invalid_argument("no differentiable kernel for the FFT size " + std::to_string(N_)); \
     }
 
 unsigned pair_grid(const DiffArgs &a)
 {
     const int64_t pairs = int64_t(a.n) * a.nwin;
-    if (pairs > int64_t(0x7fffffff)) throw std::invalid_argument("framecor: too many pairs for one launch");
-    if (a.L > 256) throw std::invalid_argument("framecor: the differentiable path holds search windows up to 256 pixels");
+    if (pairs > int64_t(0x7fffffff)) throw std::invalid_argument("too many pairs for one launch");
+    if (a.L > 256) throw std::invalid_argument("the differentiable path holds search windows up to 256 pixels");
     return unsigned(pairs);
 }
 

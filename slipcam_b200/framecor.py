@@ -255,3 +255,109 @@ def sat(frames):
     if rc != _lib.OK:
         raise ValueError('framecor: sat: invalid arguments')
     return s32.to(torch.int64) & 0xFFFFFFFF, s64
+
+
+class MultiCorrelator:
+    """
+    Several window grids (window sizes, search ranges, grids) of one video correlated together:
+    one persistent launch over every grid's (window, frame) pairs, the step captured in a CUDA
+    graph (b200 backend only; the reference correlates one grid per Correlator).
+
+    grids: a list of dicts with keys down, across, window, search (as for Correlator); up to 4.
+    correlate(frames, gross=None) takes uint8 CUDA frames (n x height x width) and, per grid, a
+    gross offset array or None, and returns one output dict per grid, as Correlator.correlate.
+    tune(frames, gross=None) picks the launch configuration by timing the candidates.
+    """
+
+    def __init__(self, height, width, grids, *, stat_size=21, device=0):
+        if not 1 <= len(grids) <= 4:
+            raise ValueError('framecor: a group holds 1 to 4 grids')
+        self._height, self._width = height, width
+        self.grids = [Correlator(height, width, g['down'], g['across'], window=g['window'], search=g['search'],
+                                 backend='b200', stat_size=stat_size, device=device) for g in grids]
+        self._g = None
+        hs = (ctypes.c_void_p * len(self.grids))(*[c._h for c in self.grids])
+        g = ctypes.c_void_p()
+        rc = _lib.lib().b200_group_create(hs, len(self.grids), ctypes.byref(g))
+        _lib.raise_for(rc, None, group=True)
+        self._g = g
+
+    def __del__(self):
+        g = getattr(self, '_g', None)
+        self._g = None
+        if g is not None and _lib is not None and _lib._lib is not None:
+            _lib._lib.b200_group_destroy(g)
+
+    def set_reference(self, frame):
+        """The reference frame of every grid."""
+        for c in self.grids:
+            c.set_reference(frame)
+
+    def _args(self, frames, gross):
+        import torch
+        if not (_is_torch(frames) and frames.is_cuda):
+            raise ValueError('framecor: MultiCorrelator takes CUDA frames')
+        if frames.dim() != 3 or frames.shape[1] != self._height or frames.shape[2] != self._width:
+            raise ValueError('framecor: the frames must be frames x height x width')
+        f = frames.to(torch.uint8).contiguous()
+        n, k = f.shape[0], len(self.grids)
+        gross = [None] * k if gross is None else list(gross)
+        if len(gross) != k:
+            raise ValueError('framecor: one gross entry per grid')
+        gs, modes, keep = [], [], []
+        for c, g in zip(self.grids, gross):
+            if g is None:
+                gs.append(None)
+                modes.append(0)
+                continue
+            t, mode = c._gross(torch.as_tensor(g), n, torch)
+            t = t.to(f.device)
+            keep.append(t)
+            gs.append(t.data_ptr())
+            modes.append(mode)
+        gp = (ctypes.c_void_p * k)(*gs)
+        mp = (ctypes.c_int * k)(*modes)
+        return f, n, gp, mp, keep
+
+    def correlate(self, frames, gross=None):
+        import torch
+        f, n, gp, mp, keep = self._args(frames, gross)
+        outs = []
+        for c in self.grids:
+            ny, nx = c.shape
+            outs.append(dict(offsets=torch.empty((n, ny, nx, 2), dtype=torch.float32, device=f.device),
+                             peak=torch.empty((n, ny, nx), dtype=torch.float32, device=f.device),
+                             snr=torch.empty((n, ny, nx), dtype=torch.float32, device=f.device),
+                             cov=torch.empty((n, ny, nx, 3), dtype=torch.float32, device=f.device)))
+        if n:
+            k = len(self.grids)
+            ptrs = {key: (ctypes.c_void_p * k)(*[o[key].data_ptr() for o in outs]) for key in ('offsets', 'peak', 'snr', 'cov')}
+            stream = torch.cuda.current_stream(f.device).cuda_stream
+            rc = _lib.lib().b200_group_correlate_device(self._g, f.data_ptr(), n, self._width, gp, mp, ptrs['offsets'],
+                                                        ptrs['peak'], ptrs['snr'], ptrs['cov'], stream)
+            _lib.raise_for(rc, self._g, group=True)
+        del keep
+        return outs
+
+    def tune(self, frames, gross=None):
+        """Time the launch configurations on these frames and keep the fastest; returns
+        (ms per launch, config)."""
+        import torch
+        f, n, gp, mp, keep = self._args(frames, gross)
+        ms = ctypes.c_double()
+        stream = torch.cuda.current_stream(f.device).cuda_stream
+        rc = _lib.lib().b200_group_tune(self._g, f.data_ptr(), n, self._width, gp, mp, stream, ctypes.byref(ms))
+        _lib.raise_for(rc, self._g, group=True)
+        del keep
+        return ms.value, self.config()
+
+    def config(self):
+        """threads per CTA, pairs per work item, costliest grid first, CUDA graph replay"""
+        t, c, f, g = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.raise_for(_lib.lib().b200_group_config(self._g, ctypes.byref(t), ctypes.byref(c), ctypes.byref(f),
+                                                   ctypes.byref(g)), self._g, group=True)
+        return dict(threads=t.value, chunk=c.value, costly_first=bool(f.value), graph=bool(g.value))
+
+    def set_config(self, threads=256, chunk=1, costly_first=True, graph=True):
+        rc = _lib.lib().b200_group_set_config(self._g, threads, chunk, int(costly_first), int(graph))
+        _lib.raise_for(rc, self._g, group=True)
