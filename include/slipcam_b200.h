@@ -147,18 +147,21 @@ B200_API int b200_group_correlate_device(b200_group *g, const uint8_t *frames, i
                                          float *const *offset, float *const *peak, float *const *snr,
                                          float *const *cov, void *stream);
 
-/* The autotuner: times the persistent launch on these frames for every candidate of threads per
- * CTA (256, 512), (window, frame) pairs per work item (1, 2, 4, 8) and grid order (costliest
- * first or as given), keeps the fastest and returns its time (ms per launch). Synchronous;
- * allocates its own temporary outputs. */
+/* The autotuner: times the whole step on these frames for every candidate of the persistent
+ * launch -- threads per CTA (256, 512), (window, frame) pairs per work item (1, 2, 4, 8), grid
+ * order (costliest first or as given) -- and for the per-grid mode (each grid's own kernel, in
+ * the same graph), keeps the fastest and returns its time (ms per step). Synchronous; allocates
+ * its own temporary outputs. */
 B200_API int b200_group_tune(b200_group *g, const uint8_t *frames, int n, int pitch,
                              const int32_t *const *gross, const int *gross_mode, void *stream,
                              double *best_ms);
 
-/* The launch configuration (threads per CTA, pairs per work item, costliest grid first, CUDA
- * graph replay), read or set. */
-B200_API int b200_group_config(const b200_group *g, int *threads, int *chunk, int *costly_first, int *use_graph);
-B200_API int b200_group_set_config(b200_group *g, int threads, int chunk, int costly_first, int use_graph);
+/* The launch configuration (threads per CTA, pairs per work item, costliest grid first, per-grid
+ * kernels instead of the persistent launch, CUDA graph replay), read or set. */
+B200_API int b200_group_config(const b200_group *g, int *threads, int *chunk, int *costly_first, int *per_grid,
+                               int *use_graph);
+B200_API int b200_group_set_config(b200_group *g, int threads, int chunk, int costly_first, int per_grid,
+                                   int use_graph);
 
 /* ---- The differentiable path: float frames, a continuous shift per pair, and the adjoints.
  * No counterpart in the reference (its backends take uint8 frames and give no derivatives); the

@@ -42,8 +42,9 @@ SIGNATURES = {
                                          ctypes.POINTER(_vp), _vp]),
     'b200_group_tune': (_i, [_vp, _u8p, _i, _i, ctypes.POINTER(_vp), ctypes.POINTER(_i), _vp,
                              ctypes.POINTER(ctypes.c_double)]),
-    'b200_group_config': (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
-    'b200_group_set_config': (_i, [_vp, _i, _i, _i, _i]),
+    'b200_group_config': (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i),
+                               ctypes.POINTER(_i)]),
+    'b200_group_set_config': (_i, [_vp, _i, _i, _i, _i, _i]),
     'b200_set_reference_f32_device': (_i, [_vp, _vp, _i, _vp]),
     'b200_diff_forward': (_i, [_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     'b200_diff_backward': (_i, [_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

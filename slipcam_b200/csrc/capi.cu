@@ -1089,6 +1089,8 @@ struct b200_group {
     size_t big_per_cta = 0;
     int nt = 256, chunk = 1;             // the launch configuration (b200_group_tune)
     bool costly_first = true, use_graph = true;
+    bool per_grid = false;               // each grid's own kernel instead of the persistent launch
+    MultiArgs host_args{};               // the arguments of the current step (per-grid mode)
     cudaGraphExec_t exec = nullptr;
     std::vector<uintptr_t> key;          // what the captured step was made for
     uint64_t launches = 0;
@@ -1194,9 +1196,26 @@ struct b200_group {
             dinv_kernel<<<dim3(unsigned((width - W + 1 + 127) / 128), unsigned(height - W + 1), unsigned(n)), 128, 0, stream>>>(
                 sat.p, sat2.p, sat_size(), height, width, W, dinv[wi].p, dinv_size(), dpitch());
         }
-        CK(cudaMemsetAsync(counter.p, 0, sizeof(int), stream));
-        launch_corr_multi(args.p, nt, smem(), grid_ctas(), stream);
+        if (per_grid) {
+            for (int i = 0; i < host_args.ngrids; ++i) {
+                const MultiGrid &G = host_args.g[host_args.order[i]];
+                if (G.N == kBigN)
+                    launch_corr_big(G.a, big.p, stream);
+                else
+                    B200_DISPATCH(G.N, launch_corr, G.a, stream);
+            }
+        } else {
+            CK(cudaMemsetAsync(counter.p, 0, sizeof(int), stream));
+            launch_corr_multi(args.p, nt, smem(), grid_ctas(), stream);
+        }
         CK(cudaGetLastError());
+    }
+
+    // the arguments of a step, on the device and here
+    void set_args(const MultiArgs &m)
+    {
+        host_args = m;
+        CK(cudaMemcpy(args.p, &m, sizeof(MultiArgs), cudaMemcpyHostToDevice));
     }
 };
 
@@ -1310,7 +1329,7 @@ int b200_group_correlate_device(b200_group *g, const uint8_t *frames, int n, int
         cudaStream_t user = static_cast<cudaStream_t>(stream);
         // what the step is made for: a captured graph stays valid while all of it is unchanged
         std::vector<uintptr_t> key = {uintptr_t(frames), uintptr_t(n), uintptr_t(pitch), uintptr_t(g->nt),
-                                      uintptr_t(g->chunk), uintptr_t(g->costly_first)};
+                                      uintptr_t(g->chunk), uintptr_t(g->costly_first), uintptr_t(g->per_grid)};
         for (size_t i = 0; i < g->grids.size(); ++i) {
             key.push_back(gross ? uintptr_t(gross[i]) : 0);
             key.push_back(gross && gross[i] ? uintptr_t(gross_mode[i]) : 0);
@@ -1320,8 +1339,7 @@ int b200_group_correlate_device(b200_group *g, const uint8_t *frames, int n, int
         CK(cudaStreamWaitEvent(g->stream, g->ev_in, 0));
         if (key != g->key) {
             CK(cudaStreamSynchronize(g->stream));   // a step in flight may still read the arguments
-            const MultiArgs m = g->make_args(frames, n, pitch, gross, gross_mode, offset, peak, snr, cov);
-            CK(cudaMemcpy(g->args.p, &m, sizeof(MultiArgs), cudaMemcpyHostToDevice));
+            g->set_args(g->make_args(frames, n, pitch, gross, gross_mode, offset, peak, snr, cov));
             if (g->use_graph) {
                 cudaGraph_t graph = nullptr;
                 CK(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
@@ -1381,36 +1399,42 @@ int b200_group_tune(b200_group *g, const uint8_t *frames, int n, int pitch, cons
         CK(cudaEventCreate(&t1));
         double best = 1e30;
         int bnt = g->nt, bchunk = g->chunk;
-        bool bfirst = g->costly_first;
+        bool bfirst = g->costly_first, bper = g->per_grid;
+        struct Cand {
+            int nt, chunk;
+            bool first, per_grid;
+        };
+        std::vector<Cand> cands;
+        for (int nt : {256, 512})
+            for (int chunk : {1, 2, 4, 8})
+                for (bool first : {true, false}) cands.push_back({nt, chunk, first, false});
+        cands.push_back({256, 1, true, true});
         try {
-            for (int nt : {256, 512})
-                for (int chunk : {1, 2, 4, 8})
-                    for (bool first : {true, false}) {
-                        g->nt = nt;
-                        g->chunk = chunk;
-                        g->costly_first = first;
-                        g->reserve(n);
-                        const MultiArgs m = g->make_args(frames, n, pitch, gross, gross_mode, off.data(), pk.data(),
-                                                         sn.data(), cv.data());
-                        CK(cudaMemcpy(g->args.p, &m, sizeof(MultiArgs), cudaMemcpyHostToDevice));
-                        g->step(frames, n, pitch);   // tables and a warm-up
-                        float ms = 0.0f, total = 0.0f;
-                        for (int r = 0; r < 3; ++r) {
-                            CK(cudaMemsetAsync(g->counter.p, 0, sizeof(int), g->stream));
-                            CK(cudaEventRecord(t0, g->stream));
-                            launch_corr_multi(g->args.p, g->nt, g->smem(), g->grid_ctas(), g->stream);
-                            CK(cudaEventRecord(t1, g->stream));
-                            CK(cudaEventSynchronize(t1));
-                            CK(cudaEventElapsedTime(&ms, t0, t1));
-                            total += ms;
-                        }
-                        if (total / 3 < best) {
-                            best = total / 3;
-                            bnt = nt;
-                            bchunk = chunk;
-                            bfirst = first;
-                        }
-                    }
+            for (const Cand &c : cands) {
+                g->nt = c.nt;
+                g->chunk = c.chunk;
+                g->costly_first = c.first;
+                g->per_grid = c.per_grid;
+                g->reserve(n);
+                g->set_args(g->make_args(frames, n, pitch, gross, gross_mode, off.data(), pk.data(), sn.data(), cv.data()));
+                g->step(frames, n, pitch);   // a warm-up
+                float ms = 0.0f, total = 0.0f;
+                for (int r = 0; r < 3; ++r) {   // the whole step: tables, denominators, correlation
+                    CK(cudaEventRecord(t0, g->stream));
+                    g->step(frames, n, pitch);
+                    CK(cudaEventRecord(t1, g->stream));
+                    CK(cudaEventSynchronize(t1));
+                    CK(cudaEventElapsedTime(&ms, t0, t1));
+                    total += ms;
+                }
+                if (total / 3 < best) {
+                    best = total / 3;
+                    bnt = c.nt;
+                    bchunk = c.chunk;
+                    bfirst = c.first;
+                    bper = c.per_grid;
+                }
+            }
         } catch (...) {
             cudaEventDestroy(t0);
             cudaEventDestroy(t1);
@@ -1422,22 +1446,24 @@ int b200_group_tune(b200_group *g, const uint8_t *frames, int n, int pitch, cons
         g->nt = bnt;
         g->chunk = bchunk;
         g->costly_first = bfirst;
+        g->per_grid = bper;
         g->key.clear();
         if (best_ms) *best_ms = best;
     });
 }
 
-int b200_group_config(const b200_group *g, int *threads, int *chunk, int *costly_first, int *use_graph)
+int b200_group_config(const b200_group *g, int *threads, int *chunk, int *costly_first, int *per_grid, int *use_graph)
 {
     if (!g) return B200_EINVAL;
     if (threads) *threads = g->nt;
     if (chunk) *chunk = g->chunk;
     if (costly_first) *costly_first = g->costly_first;
+    if (per_grid) *per_grid = g->per_grid;
     if (use_graph) *use_graph = g->use_graph;
     return B200_OK;
 }
 
-int b200_group_set_config(b200_group *g, int threads, int chunk, int costly_first, int use_graph)
+int b200_group_set_config(b200_group *g, int threads, int chunk, int costly_first, int per_grid, int use_graph)
 {
     return guarded_group(g, [&] {
         if ((threads != 256 && threads != 512) || chunk < 1 || chunk > 64)
@@ -1445,6 +1471,7 @@ int b200_group_set_config(b200_group *g, int threads, int chunk, int costly_firs
         g->nt = threads;
         g->chunk = chunk;
         g->costly_first = costly_first != 0;
+        g->per_grid = per_grid != 0;
         g->use_graph = use_graph != 0;
         g->key.clear();
     });

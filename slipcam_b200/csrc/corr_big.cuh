@@ -3,7 +3,7 @@
 //
 // The passes of fft_passes.cuh run on pieces of the spectrum, staged through a per-CTA scratch
 // in global memory (it stays in L2: 148 CTAs x 397 KB = 59 MB):
-//   1. row pass in chunks of 16 rows: chip rows -> shared memory -> row_forward -> the rows' half
+//   1. row pass in chunks of 32 rows: chip rows -> shared memory -> row_forward -> the rows' half
 //      spectra to the scratch (Lr x NH)
 //   2. column pass in two halves of the NH columns: a half (N rows x <= 65 columns) -> shared
 //      memory -> col_pass (forward, x conj(reference spectrum), inverse, rows [0, M) kept) -> the
@@ -24,7 +24,7 @@ struct BigGeo {
     static constexpr int NH = G::NH, NHP = G::NHP, RP = G::RP;
     static constexpr int H0 = (NH + 1) / 2;                     // columns of the first half
     static constexpr int WS = H0 + 1;                           // their stride in shared memory
-    static constexpr int CHUNK = 16;                            // rows per row-pass chunk
+    static constexpr int CHUNK = 32;                            // rows per row-pass chunk
     static constexpr size_t work_bytes = size_t(N) * WS * sizeof(float2);
     static constexpr size_t smem_bytes = work_bytes + 2 * N * sizeof(float2);
     // the inverse row pass on M rows uses complex rows up to (M rounded up to even - 2) plus an
@@ -47,6 +47,7 @@ __device__ void big_rows(float2 *W, const float2 *TW, int Lr, int L, float2 *gs,
     float *Sr = reinterpret_cast<float *>(W);
     for (int r0 = 0; r0 < Lr; r0 += B::CHUNK) {
         const int rows = min(B::CHUNK, Lr - r0);
+#pragma unroll 8
         for (int idx = threadIdx.x; idx < rows * N; idx += NT) {
             const int i = idx / N, j = idx % N;
             Sr[size_t(i) * B::RP + j] = (r0 + i < L && j < L) ? row(r0 + i, j) : 0.0f;
@@ -54,6 +55,7 @@ __device__ void big_rows(float2 *W, const float2 *TW, int Lr, int L, float2 *gs,
         __syncthreads();
         row_forward<N>(ex, W, rows / 2, TW);
         __syncthreads();
+#pragma unroll 4
         for (int idx = threadIdx.x; idx < rows * B::NH; idx += NT) {
             const int i = idx / B::NH, k = idx % B::NH;
             gs[size_t(r0 + i) * B::NH + k] = W[size_t(i) * B::NHP + k];
@@ -72,6 +74,7 @@ __device__ void big_cols(float2 *W, const float2 *TW, const float2 *TWI, int Lr,
     const DevExec ex{int(threadIdx.x >> 5), NT / 32};
     for (int h = 0; h < 2; ++h) {
         const int k0 = h ? B::H0 : 0, nc = h ? B::NH - B::H0 : B::H0;
+#pragma unroll 8
         for (int idx = threadIdx.x; idx < Lr * nc; idx += NT) {
             const int r = idx / nc, c = idx % nc;
             W[size_t(r) * B::WS + c] = gs[size_t(r) * B::NH + k0 + c];
@@ -189,6 +192,7 @@ __device__ void corr_big_pair(const CorrArgs &a, int p, float2 *W, float2 *gs)
     big_rows<N, NT>(W, TW, Lr, L, gs, [&](int i, int j) { return float(__ldg(chip + int64_t(i) * a.pitch + j)) - mean; });
     big_cols<N, NT, true>(W, TW, TWI, Lr, M, gs, a.spec + size_t(k) * B::NH * N, nullptr, gm);
     // rows [0, M) of the column-inverted spectrum, whole again, then the inverse row pass
+#pragma unroll 8
     for (int idx = threadIdx.x; idx < M * B::NH; idx += NT) {
         const int u = idx / B::NH, c = idx % B::NH;
         W[size_t(u) * B::NHP + c] = gm[size_t(u) * B::NH + c];

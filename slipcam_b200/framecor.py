@@ -352,12 +352,14 @@ class MultiCorrelator:
         return ms.value, self.config()
 
     def config(self):
-        """threads per CTA, pairs per work item, costliest grid first, CUDA graph replay"""
-        t, c, f, g = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        """threads per CTA, pairs per work item, costliest grid first, per-grid kernels instead of
+        the persistent launch, CUDA graph replay"""
+        t, c, f, pg, g = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _lib.raise_for(_lib.lib().b200_group_config(self._g, ctypes.byref(t), ctypes.byref(c), ctypes.byref(f),
-                                                   ctypes.byref(g)), self._g, group=True)
-        return dict(threads=t.value, chunk=c.value, costly_first=bool(f.value), graph=bool(g.value))
+                                                   ctypes.byref(pg), ctypes.byref(g)), self._g, group=True)
+        return dict(threads=t.value, chunk=c.value, costly_first=bool(f.value), per_grid=bool(pg.value),
+                    graph=bool(g.value))
 
-    def set_config(self, threads=256, chunk=1, costly_first=True, graph=True):
-        rc = _lib.lib().b200_group_set_config(self._g, threads, chunk, int(costly_first), int(graph))
+    def set_config(self, threads=256, chunk=1, costly_first=True, per_grid=False, graph=True):
+        rc = _lib.lib().b200_group_set_config(self._g, threads, chunk, int(costly_first), int(per_grid), int(graph))
         _lib.raise_for(rc, self._g, group=True)

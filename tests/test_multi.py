@@ -77,7 +77,8 @@ def test_group_graph_replay_and_configs():
     want2 = singles(ref, frames2, gross)
     for a, b in zip(second, want2):
         same(a, b)
-    for cfg in (dict(threads=512, chunk=4, costly_first=False, graph=False), dict(threads=256, chunk=8, graph=True)):
+    for cfg in (dict(threads=512, chunk=4, costly_first=False, graph=False), dict(threads=256, chunk=8, graph=True),
+                dict(per_grid=True, graph=True), dict(per_grid=True, graph=False)):
         mc.set_config(**cfg)
         buf.copy_(torch.as_tensor(frames))
         again = mc.correlate(buf, gross=g)
