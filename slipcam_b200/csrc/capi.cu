@@ -212,8 +212,12 @@ void launch_corr_tc(const CorrArgs &a, const uint4 *dtab, int *status, const CUt
 template <int N>
 bool tc_fits_n(int M)
 {
-    // the surface (A region, M x M floats) and the box of variance denominators (X region)
-    return size_t(M) * M * 4 <= TcGeo<N>::A_BYTES && size_t(tc_box_width(M)) * M * 4 <= TcGeo<N>::X_BYTES;
+    // the box of variance denominators (X region), and the S5 result in the top NO TMEM columns
+    // clear of every other stage's accumulators
+    using G = TcGeo<N>;
+    const int NO = (M + 15) / 16 * 16;
+    const int used = std::max({2 * G::KP * G::T1, 2 * N, 2 * NO});
+    return size_t(tc_box_width(M)) * M * 4 <= G::X_BYTES && used + NO <= int(G::TMEM_COLS);
 }
 
 // whether the tensor-core kernel holds this geometry: FFT size up to 160, up to 128 shifts per axis

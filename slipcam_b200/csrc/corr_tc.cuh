@@ -79,14 +79,22 @@ __device__ __forceinline__ uint4 pack8(const float *v)
     return r;
 }
 
-// the MMAs of the current phase have completed: one thread polls the mbarrier, the others wait at
-// the barrier; false (for all threads) if the poll gave up
-__device__ __forceinline__ bool tc_wait_all(uint64_t *mbar, uint32_t &phase)
+// eight compute warps, two per TMEM lane quadrant (warp w and w + 4 own the same 32 accumulator rows
+// and split their columns), and a control warp whose first thread issues the MMAs and the TMA
+// copies, polls their completion and does the per-pair scalar work, so that no compute warp waits
+// behind the tensor core's issue queue
+constexpr int kTcCompute = 8;
+constexpr int kTcThreads = 32 * (kTcCompute + 1);
+constexpr int kTcCtrl = 32 * kTcCompute;   // the control thread
+
+// the MMAs of the current phase have completed: the control thread polls the mbarrier, the others
+// wait at the barrier; false (for all threads) if the poll gave up or any thread passes also_failed
+__device__ __forceinline__ bool tc_wait_all(uint64_t *mbar, uint32_t &phase, bool also_failed = false)
 {
     bool ok = true;
-    if (threadIdx.x == 0) ok = tc::mbar_wait(mbar, phase);
+    if (threadIdx.x == kTcCtrl) ok = tc::mbar_wait(mbar, phase);
     phase ^= 1u;
-    const bool failed = __syncthreads_or(!ok);
+    const bool failed = __syncthreads_or(!ok || also_failed);
     tc::fence_after_sync();
     return !failed;
 }
@@ -121,9 +129,6 @@ struct PairSetup {
     bool ok;                // the chip lies inside the frame and the reference window has texture
 };
 
-// two warps per TMEM lane quadrant: warp w and w + 4 own the same 32 accumulator rows and split
-// their columns
-constexpr int kTcThreads = 256;
 
 // the rows of the variance-denominator box a TMA copy brings in: x rounded down to 4 floats
 // (16 bytes), so BW = M + 3 rounded up to 4 floats per row
@@ -137,7 +142,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
 {
     using G = TcGeo<N>;
     constexpr int NH = G::NH, KP = G::KP, NT = kTcThreads;
-    constexpr bool kPeakInS3 = KP <= 3 * 32;   // TMEM lanes 96 .. 127 (the last warp's) hold no kappa row
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ uint32_t tmem_base;
     __shared__ __align__(8) uint64_t mbar, tbar;
@@ -149,8 +153,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int quad = warp & 3, half = warp >> 2;
     const int row = 32 * quad + lane;   // this thread's accumulator row (TMEM lane)
+    const bool compute = warp < kTcCompute, ctrl = tid == kTcCtrl;
     unsigned char *A = smem, *X = smem + G::OFF_X;
-    float *surf = reinterpret_cast<float *>(A);        // the surface, after S5 (A region)
     float *dvs = reinterpret_cast<float *>(X);         // the variance denominators, from S2 on (X region)
     const uint32_t sA = tc::smem_u32(A), sX = tc::smem_u32(X);
     const uint32_t sDR = tc::smem_u32(smem + G::OFF_DR), sDI = tc::smem_u32(smem + G::OFF_DI);
@@ -159,7 +163,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
     for (int i = tid; i < int(2 * G::D_BYTES / 16); i += NT)
         reinterpret_cast<uint4 *>(smem + G::OFF_DR)[i] = __ldg(dtab + i);
     if (warp == 0) tc::tmem_alloc(&tmem_base, G::TMEM_COLS);
-    if (tid == 0) {
+    if (ctrl) {
         tc::mbar_init(&mbar, 1);
         tc::mbar_init(&tbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -182,33 +186,24 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
     const size_t ss = size_t(a.w) + 1;
     const bool words = ((a.pitch | reinterpret_cast<uintptr_t>(a.frames) | int(a.fstride)) & 3) == 0;
 
-    // the pair whose peak the last warp still has to write, from its 3 x 3 neighbourhood (s_fit) and
-    // the SNR patch's sums of squares (s_sq, one per warp), in the next pair's S3 (where the last
-    // warp has no kappa rows) or else its S1
-    struct Pending {
+    // the pair whose epilogue is pending: its S5 result in TMEM columns [C5, C5 + NO) while the next
+    // pair runs S1 .. S4; its variance denominators come by TMA into the X region after the next
+    // pair's S1, the normalization and argmax run during its S2, the SNR patch and the 3 x 3 fit
+    // values (read back from TMEM) during its S4, the FP64 peak solve during its S5
+    struct Prev {
         int64_t q;
-        int at, gy, gx;
-        bool valid, live;
-    } pend{0, 0, 0, 0, false, false};
-    auto finish_peak = [&](Pending &pp) {
-        if (!pp.live) return;
-        pp.live = false;
-        if (lane != 0) return;
-        if (!pp.valid) {
-            invalid_outputs(pp.q, a.offset, a.peak, a.snr, a.cov);
-            return;
-        }
-        const int u = pp.at / M, v = pp.at % M;
-        int i0, i1, j0, j1;
-        snr_patch(M, a.stat, u, v, i0, i1, j0, j1);
-        double sum = 0.0;
-        for (int w = 0; w < NT / 32; ++w) sum += s_sq[w];
-        peak_outputs(s_fit + 4, 3, M, u, v, R, pp.gy, pp.gx, W * W, sum, (i1 - i0) * (j1 - j0), pp.q, a.offset, a.peak,
-                     a.snr, a.cov);
-    };
+        int f, sy, sx, gy, gx;
+        float scale;
+        bool live;
+    } prev{0, 0, 0, 0, 0, 0, 0.0f, false};
+    const uint32_t C5 = uint32_t(G::TMEM_COLS - NO);
+    float e_best = -2.0f;   // this thread's running argmax of the pending pair
+    int e_at = INT_MAX;
+    bool e_valid = false;   // the pending pair's surface has a positive peak
+    int e_pu = 0, e_pv = 0;
 
     // the next pair's window, frame, position and chip mean, worked out by one thread of the last
-    // warp while the tensor cores run S2 (global-memory latency off the gather's path)
+    // warp while the tensor cores run S1 (global-memory latency off the gather's path)
     auto pair_setup = [&](int p) {
         PairSetup o{};
         o.p = p;
@@ -236,96 +231,235 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
         }
         return o;
     };
-    if (tid == NT - 32) s_next = pair_setup(blockIdx.x);
-    __syncthreads();
 
-    for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
-        const PairSetup cur = s_next;
-        const int k = cur.k, f = cur.f, sy = cur.sy, sx = cur.sx;
-        const int64_t q = cur.q;
-        const float norm = cur.norm;
-        if (!cur.ok) {
-            if (tid == 0) invalid_outputs(q, a.offset, a.peak, a.snr, a.cov);
-            if (a.surface)
-                for (int i = tid; i < M * M; i += NT) a.surface[q * M * M + i] = 0.0f;
-            __syncthreads();   // every thread has read s_next
-            if (tid == NT - 32) s_next = pair_setup(p + gridDim.x);
-            __syncthreads();
-            continue;
-        }
-
-        // ---- X = chip - round(mean), FP16, K-major (rows i, columns j), zero outside L x L. A warp
-        // takes 8 rows x 4 chunks of 8 pixels: 32-byte pieces of 8 rows from global memory, one
-        // contiguous 512-byte store into shared memory. Every load of the thread first.
-        const __half2 off = __float2half2_rn(1024.0f + float(cur.mean));
-        const uint8_t *chip = a.frames + f * a.fstride + int64_t(sy) * a.pitch + sx;
-        {
-            constexpr int NCG = (N / 8 + 3) / 4;               // groups of 4 chunks per row
-            constexpr int NB = (N / 8) * NCG;                   // blocks of 8 rows x 4 chunks
-            constexpr int PERT = (NB + NT / 32 - 1) / (NT / 32);   // blocks per warp
-            constexpr int PERW = (PERT + 1) / 2;                    // in two rounds
-#pragma unroll
-            for (int round = 0; round < 2; ++round) {
-            uint32_t w0[PERW], w1[PERW], w2[PERW];
-#pragma unroll
-            for (int t = 0; t < PERW; ++t) {
-                const int b = warp + (NT / 32) * (t + round * PERW);
-                const int i = 8 * (b / NCG) + (lane & 7), j0 = 8 * (4 * (b % NCG) + (lane >> 3));
-                w0[t] = w1[t] = w2[t] = 0u;
-                if (b < NB && t + round * PERW < PERT && i < L && j0 < L && j0 < N) {
-                    const uint8_t *src = chip + int64_t(i) * a.pitch + j0;
-                    const int left = L - j0;   // chip bytes from src on
-                    if (words) {
-                        // the aligned words holding the chip bytes among src[0 .. 8)
-                        const uintptr_t addr = reinterpret_cast<uintptr_t>(src);
-                        const uint32_t *wp = reinterpret_cast<const uint32_t *>(addr & ~uintptr_t(3));
-                        const int sh = int(addr & 3);
-                        w0[t] = __ldg(wp);
-                        if (4 - sh < left) w1[t] = __ldg(wp + 1);
-                        if (sh > 0 && 8 - sh < left) w2[t] = __ldg(wp + 2);
-                    } else {
-                        for (int e = 0; e < 8 && e < left; ++e) {
-                            const uint32_t bt = __ldg(src + e);
-                            if (e < 4) w0[t] |= bt << (8 * e);
-                            else w1[t] |= bt << (8 * (e - 4));
-                        }
-                    }
-                }
-            }
-#pragma unroll
-            for (int t = 0; t < PERW; ++t) {
-                const int b = warp + (NT / 32) * (t + round * PERW);
-                const int i = 8 * (b / NCG) + (lane & 7), j0 = 8 * (4 * (b % NCG) + (lane >> 3));
-                if (b < NB && t + round * PERW < PERT && j0 < N) {
-                    uint4 out = make_uint4(0u, 0u, 0u, 0u);
-                    if (i < L && j0 < L) {
-                        uint32_t lo = w0[t], hi = w1[t];
+    // ---- X = chip - round(mean), FP16, K-major (rows i, columns j), zero outside L x L. A warp
+    // takes 8 rows x 4 chunks of 8 pixels: 32-byte pieces of 8 rows from global memory, one
+    // contiguous 512-byte store into shared memory. Every load of the thread first.
+    auto gather = [&](const PairSetup &c) {
+        if (!compute) return;
+        const __half2 off = __float2half2_rn(1024.0f + float(c.mean));
+        const uint8_t *chip = a.frames + c.f * a.fstride + int64_t(c.sy) * a.pitch + c.sx;
+            {
+                constexpr int NCG = (N / 8 + 3) / 4;               // groups of 4 chunks per row
+                constexpr int NB = (N / 8) * NCG;                   // blocks of 8 rows x 4 chunks
+                constexpr int PERT = (NB + kTcCompute - 1) / kTcCompute;   // blocks per warp
+                constexpr int PERW = (PERT + 1) / 2;                    // in two rounds
+    #pragma unroll
+                for (int round = 0; round < 2; ++round) {
+                uint32_t w0[PERW], w1[PERW], w2[PERW];
+    #pragma unroll
+                for (int t = 0; t < PERW; ++t) {
+                    const int b = warp + kTcCompute * (t + round * PERW);
+                    const int i = 8 * (b / NCG) + (lane & 7), j0 = 8 * (4 * (b % NCG) + (lane >> 3));
+                    w0[t] = w1[t] = w2[t] = 0u;
+                    if (b < NB && t + round * PERW < PERT && i < L && j0 < L && j0 < N) {
+                        const uint8_t *src = chip + int64_t(i) * a.pitch + j0;
+                        const int left = L - j0;   // chip bytes from src on
                         if (words) {
-                            const int sh = int(reinterpret_cast<uintptr_t>(chip + int64_t(i) * a.pitch + j0) & 3);
-                            lo = __funnelshift_r(w0[t], w1[t], 8 * sh);
-                            hi = __funnelshift_r(w1[t], w2[t], 8 * sh);
-                        }
-                        bytes_to_half(lo, off, out.x, out.y);
-                        bytes_to_half(hi, off, out.z, out.w);
-                        if (j0 + 8 > L) {   // the last chunk of a row: zero past the chip
-                            const int keep = L - j0;   // 1 .. 7 pixels
-                            uint32_t *o = reinterpret_cast<uint32_t *>(&out);
-#pragma unroll
-                            for (int e = 0; e < 4; ++e) {
-                                if (2 * e >= keep) o[e] = 0u;
-                                else if (2 * e + 1 >= keep) o[e] &= 0xFFFFu;
+                            // the aligned words holding the chip bytes among src[0 .. 8)
+                            const uintptr_t addr = reinterpret_cast<uintptr_t>(src);
+                            const uint32_t *wp = reinterpret_cast<const uint32_t *>(addr & ~uintptr_t(3));
+                            const int sh = int(addr & 3);
+                            w0[t] = __ldg(wp);
+                            if (4 - sh < left) w1[t] = __ldg(wp + 1);
+                            if (sh > 0 && 8 - sh < left) w2[t] = __ldg(wp + 2);
+                        } else {
+                            for (int e = 0; e < 8 && e < left; ++e) {
+                                const uint32_t bt = __ldg(src + e);
+                                if (e < 4) w0[t] |= bt << (8 * e);
+                                else w1[t] |= bt << (8 * (e - 4));
                             }
                         }
                     }
-                    *reinterpret_cast<uint4 *>(X + tc::k_major_offset(i, j0, G::SBO_D, 128)) = out;
+                }
+    #pragma unroll
+                for (int t = 0; t < PERW; ++t) {
+                    const int b = warp + kTcCompute * (t + round * PERW);
+                    const int i = 8 * (b / NCG) + (lane & 7), j0 = 8 * (4 * (b % NCG) + (lane >> 3));
+                    if (b < NB && t + round * PERW < PERT && j0 < N) {
+                        uint4 out = make_uint4(0u, 0u, 0u, 0u);
+                        if (i < L && j0 < L) {
+                            uint32_t lo = w0[t], hi = w1[t];
+                            if (words) {
+                                const int sh = int(reinterpret_cast<uintptr_t>(chip + int64_t(i) * a.pitch + j0) & 3);
+                                lo = __funnelshift_r(w0[t], w1[t], 8 * sh);
+                                hi = __funnelshift_r(w1[t], w2[t], 8 * sh);
+                            }
+                            bytes_to_half(lo, off, out.x, out.y);
+                            bytes_to_half(hi, off, out.z, out.w);
+                            if (j0 + 8 > L) {   // the last chunk of a row: zero past the chip
+                                const int keep = L - j0;   // 1 .. 7 pixels
+                                uint32_t *o = reinterpret_cast<uint32_t *>(&out);
+    #pragma unroll
+                                for (int e = 0; e < 4; ++e) {
+                                    if (2 * e >= keep) o[e] = 0u;
+                                    else if (2 * e + 1 >= keep) o[e] &= 0xFFFFu;
+                                }
+                            }
+                        }
+                        *reinterpret_cast<uint4 *>(X + tc::k_major_offset(i, j0, G::SBO_D, 128)) = out;
+                    }
+                }
                 }
             }
+        tc::fence_smem_async();   // the chip is read by the tensor core
+    };
+
+    // ---- the pending pair's epilogue, in three parts (all threads call each)
+    // the denominator box (rows sy .. sy + M - 1, columns from sx rounded down to 4) into X
+    bool tma_pending = false;   // a denominator box is on its way (waited out before leaving)
+    auto epi_fetch = [&]() {
+        if (ctrl) {
+            tc::mbar_expect_tx(&tbar, uint32_t(BW * M * 4));
+            tc::tma_load_3d(dvs, dmap, prev.sx & ~3, prev.sy, prev.f, &tbar);
+        }
+        tma_pending = true;
+    };
+    // the normalized surface (thread v holds column v) and this thread's argmax; 16-column chunks
+    // of u alternate between the two warps of a quadrant. false if the box did not arrive.
+    auto epi_normalize = [&]() -> bool {
+        const bool ok = tc::mbar_wait(&tbar, tphase);
+        tphase ^= 1u;
+        tma_pending = !ok;
+        e_best = -2.0f;
+        e_at = INT_MAX;
+        if (compute && 32 * quad < M) {
+            const int v = row;
+            const bool vin = v < M;
+            const float *__restrict__ dv = dvs + (prev.sx & 3) + v;
+            float *sv = a.surface ? a.surface + prev.q * M * M + v : nullptr;
+            for (int u0 = 16 * half; u0 < NO; u0 += 32) {   // one 16-column chunk of u per TMEM wait
+                uint32_t cr[16];
+                tc::tmem_ld16_nowait(tmem + lane_base + C5 + uint32_t(u0), cr);
+                const int nu = M - u0 < 16 ? M - u0 : 16;   // rows u of the chunk inside the surface
+                float rho[16];
+#pragma unroll
+                for (int e = 0; e < 16; ++e) rho[e] = vin && e < nu ? dv[(u0 + e) * BW] : 0.0f;
+                tc::tmem_wait();
+#pragma unroll
+                for (int e = 0; e < 16; ++e) rho[e] *= __uint_as_float(cr[e]) * prev.scale;
+                if (vin) {
+                    if (sv) {
+#pragma unroll
+                        for (int e = 0; e < 16; ++e)
+                            if (e < nu) sv[(u0 + e) * M] = rho[e];
+                    }
+#pragma unroll
+                    for (int e = 0; e < 16; ++e)   // values <= -2 and NaN never win; ties keep the first u
+                        if (e < nu && rho[e] > e_best) {
+                            e_best = rho[e];
+                            e_at = u0 + e;
+                        }
+                }
+            }
+            e_at = e_at == INT_MAX ? INT_MAX : e_at * M + v;
+        }
+        return ok;
+    };
+    // the surface's argmax (the first in raster order if equal), then the SNR patch's sum of squares
+    // and the 3 x 3 fit's values, read back from TMEM with the same arithmetic
+    auto epi_peak = [&]() {
+        float best = e_best;
+        int at = e_at;
+        for (int o = 16; o > 0; o >>= 1) better(best, at, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, at, o));
+        if (lane == 0) {
+            s_best[warp] = best;
+            s_at[warp] = at;
+        }
+        __syncthreads();
+        best = lane < NT / 32 ? s_best[lane] : -2.0f;
+        at = lane < NT / 32 ? s_at[lane] : INT_MAX;
+        for (int o = 16; o > 0; o >>= 1) better(best, at, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, at, o));
+        e_valid = best > 0;
+        double sq = 0.0;
+        if (e_valid) {
+            e_pu = at / M;
+            e_pv = at % M;
+            int i0, i1, j0, j1;
+            snr_patch(M, a.stat, e_pu, e_pv, i0, i1, j0, j1);
+            // the warp pair of a quadrant takes alternate 16-row chunks of u from i0
+            if (compute && 32 * quad < j1 && 32 * quad + 32 > j0) {   // warp-uniform
+                for (int c0 = i0 + 16 * half; c0 < i1; c0 += 32) {
+                    const int cb = c0 + 16 <= NO ? c0 : NO - 16;   // 16 columns inside [0, NO)
+                    uint32_t cr[16];
+                    tc::tmem_ld16_nowait(tmem + lane_base + C5 + uint32_t(cb), cr);
+                    tc::tmem_wait();
+                    const int v = row;
+                    if (v >= j0 && v < j1) {
+                        const float *__restrict__ dv = dvs + (prev.sx & 3) + v;
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) {
+                            const int u = cb + e;
+                            if (u < c0 || u >= i1 || u >= c0 + 16) continue;
+                            float rho = dv[u * BW];
+                            rho *= __uint_as_float(cr[e]) * prev.scale;
+                            sq += double(rho) * double(rho);
+                            const int du = u - e_pu, dvv = v - e_pv;
+                            if (du >= -1 && du <= 1 && dvv >= -1 && dvv <= 1) s_fit[(du + 1) * 3 + dvv + 1] = rho;
+                        }
+                    }
+                }
             }
         }
-        tc_publish();
+        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+        if (lane == 0) s_sq[warp] = sq;
+    };
+    // the FP64 peak solve and the outputs (one thread), from s_fit and s_sq
+    auto epi_finish = [&]() {
+        if (!e_valid) {
+            invalid_outputs(prev.q, a.offset, a.peak, a.snr, a.cov);
+            return;
+        }
+        int i0, i1, j0, j1;
+        snr_patch(M, a.stat, e_pu, e_pv, i0, i1, j0, j1);
+        double sum = 0.0;
+        for (int w = 0; w < NT / 32; ++w) sum += s_sq[w];
+        peak_outputs(s_fit + 4, 3, M, e_pu, e_pv, R, prev.gy, prev.gx, W * W, sum, (i1 - i0) * (j1 - j0), prev.q,
+                     a.offset, a.peak, a.snr, a.cov);
+    };
+    // the whole epilogue of the pending pair, not overlapped (before a gather that needs X, and at
+    // the end); false if a wait gave up
+    auto epi_flush = [&]() -> bool {
+        if (!prev.live) return true;
+        epi_fetch();
+        const bool ok = epi_normalize();
+        epi_peak();
+        __syncthreads();
+        if (ctrl) epi_finish();
+        prev.live = false;
+        return !__syncthreads_or(!ok);
+    };
+
+    if (ctrl) s_next = pair_setup(blockIdx.x);
+    __syncthreads();
+    PairSetup cur = s_next;
+    if (cur.p < npairs && cur.ok) gather(cur);
+    tc_publish();
+    bool failed = false;
+    while (cur.p < npairs) {
+        if (!cur.ok) {   // an invalid pair: its outputs now (the pending epilogue waits)
+            if (ctrl) invalid_outputs(cur.q, a.offset, a.peak, a.snr, a.cov);
+            if (a.surface)
+                for (int i = tid; i < M * M; i += NT) a.surface[cur.q * M * M + i] = 0.0f;
+            if (ctrl) s_next = pair_setup(cur.p + gridDim.x);
+            __syncthreads();
+            cur = s_next;
+            __syncthreads();
+            if (cur.p < npairs && cur.ok) {
+                if (!epi_flush()) {
+                    failed = true;
+                    break;
+                }
+                gather(cur);
+                tc_publish();
+            }
+            continue;
+        }
+        const int k = cur.k;
+        const float norm = cur.norm;
 
         // ---- S1: Y = X [Dr | Di], tile t of 128 chip rows -> TMEM columns [2 KP t, 2 KP (t + 1))
-        if (tid == 0) {
+        if (ctrl) {
             B200_TC_DESCS
             const uint32_t id = tc::instr_desc(128, KP, false, false, false, false);
 #pragma unroll
@@ -339,14 +473,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
             }
             tc::mma_commit(&mbar);
         }
-        if (!kPeakInS3 && warp == NT / 32 - 1) finish_peak(pend);   // the previous pair's peak, while S1 runs
+        if (tid == kTcCtrl - 32) s_next = pair_setup(cur.p + gridDim.x);   // a compute warp, idle during S1
         if (!tc_wait_all(&mbar, phase)) {
-            if (tid == 0 && status) atomicExch(status, 3);
+            failed = true;
             break;
         }
         // S1 -> A2 (MN-major: m = kappa, k = part * N + i); warps w and w + 4 take Re and Im
         for (int t = 0; t < G::T1; ++t) {
-            if (128 * t + 32 * quad >= N) continue;   // warp-uniform
+            if (!compute || 128 * t + 32 * quad >= N) continue;   // warp-uniform
             const int i = 128 * t + row;
 #pragma unroll
             for (int cb = 0; cb < KP; cb += 16 * (KP % 32 ? 1 : 2)) {   // 32 (or 16) columns per wait
@@ -362,8 +496,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
         }
         tc_publish();
 
+        // the pending pair's denominators into X (free: S1 has read the chip)
+        if (prev.live) epi_fetch();
         // ---- S2: Z^T = Y^T D: Zr in TMEM columns [0, N), Zi in [N, 2N)
-        if (tid == 0) {
+        if (ctrl) {
             B200_TC_DESCS
             const uint32_t id = tc::instr_desc(128, N, true, false, false, false);
             const uint32_t idn = tc::instr_desc(128, N, true, false, false, true);
@@ -377,27 +513,21 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
             }
             tc::mma_commit(&mbar);
         }
-        // meanwhile: the variance denominators of this pair into the X region (free after S1)
-        // (one TMA box: rows sy .. sy + M - 1, columns from sx rounded down to 4)
-        if (tid == 0) {
-            tc::mbar_expect_tx(&tbar, uint32_t(BW * M * 4));
-            tc::tma_load_3d(dvs, dmap, sx & ~3, sy, f, &tbar);
-        }
-        if (tid == NT - 32) s_next = pair_setup(p + gridDim.x);   // read after S2's barrier
-        // and this thread's row of the reference spectrum (S3): frequency pairs (ky, ky + 1) of the
+        // this thread's row of the reference spectrum (S3): frequency pairs (ky, ky + 1) of the
         // rows kappa side by side, KP float4 per pair (rows NH .. KP - 1 zero)
         int eR = 0;
         frexpf(float(W) * norm, &eR);   // W * norm < 2^eR, and max |R| <= W * norm
         const int kap = row;
         const float4 *rrow = a.spec_tc + size_t(k) * (N / 2) * KP + (kap < KP ? kap : 0);
-        if (!tc_wait_all(&mbar, phase)) {
-            if (tid == 0 && status) atomicExch(status, 3);
+        const bool tma_ok = prev.live ? epi_normalize() : true;   // while the tensor cores run S2
+        if (!tc_wait_all(&mbar, phase, !tma_ok)) {
+            failed = true;
             break;
         }
 
         // ---- S3: P = Z conj(R) 2^-(eR + 8) -> A4 (K-major: row kappa, k = part * N + ky); the
         // 16-column chunks of ky alternate between the two warps of a quadrant
-        if (32 * quad < KP) {
+        if (compute && 32 * quad < KP) {
             const float sc = ldexpf(1.0f, -(eR + 8));
             float4 rn[8];
 #pragma unroll
@@ -434,13 +564,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
                     }
                 }
             }
-        } else if (kPeakInS3 && warp == NT / 32 - 1) {
-            finish_peak(pend);   // the previous pair's peak
         }
         tc_publish();
 
         // ---- S4: Q^T = P^T conj(D) for u < NO: Qr in TMEM columns [0, NO), Qi in [NO, 2 NO)
-        if (tid == 0) {
+        if (ctrl) {
             B200_TC_DESCS
             const uint32_t id = tc::instr_desc(128, NO, false, false, false, false);
             const uint32_t idn = tc::instr_desc(128, NO, false, false, false, true);
@@ -454,13 +582,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
             }
             tc::mma_commit(&mbar);
         }
+        if (prev.live) epi_peak();   // while the tensor cores run S4
         if (!tc_wait_all(&mbar, phase)) {
-            if (tid == 0 && status) atomicExch(status, 3);
+            failed = true;
             break;
         }
         // S4 -> B5 in the A region (MN-major: n = u, k = part * KP + kappa), with the Hermitian
         // weights and 2^-9; warps w and w + 4 take Qr and Qi
-        if (32 * quad < KP) {
+        if (compute && 32 * quad < KP) {
             const int kap = row;
             const float wgt = kap >= NH ? 0.0f : ((kap == 0 || 2 * kap == N) ? 1.0f : 2.0f) * (1.0f / 512.0f);
             for (int c0 = 0; c0 < NO; c0 += 32) {
@@ -482,95 +611,31 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
         }
         tc_publish();
 
-        // ---- S5: c^T[v][u] = sum_kappa Dr[v][kappa] B5re[kappa][u] + Di[v][kappa] B5im[kappa][u]
-        if (tid == 0) {
+        // ---- S5: c^T[v][u] = sum_kappa Dr[v][kappa] B5re[kappa][u] + Di[v][kappa] B5im[kappa][u], into
+        // TMEM columns [C5, C5 + NO), which no other stage writes: the epilogue reads it during the next pair
+        if (ctrl) {
             B200_TC_DESCS
             const uint32_t id = tc::instr_desc(128, NO, false, true, false, false);
 #pragma unroll 2
             for (int s = 0; s < KP / 16; ++s) {
-                tc::mma_f16(tmem, dR0 + 16u * s, b0B5 + 16u * s, id, s > 0);
-                tc::mma_f16(tmem, dI0 + 16u * s, b0B5 + uint32_t(KP + 16 * s), id, 1);
+                tc::mma_f16(tmem + C5, dR0 + 16u * s, b0B5 + 16u * s, id, s > 0);
+                tc::mma_f16(tmem + C5, dI0 + 16u * s, b0B5 + uint32_t(KP + 16 * s), id, 1);
             }
             tc::mma_commit(&mbar);
         }
-        if (tid == 0 && !tc::mbar_wait(&tbar, tphase) && status) atomicExch(status, 3);   // the denominators
-        tphase ^= 1u;
+        if (prev.live && ctrl) epi_finish();   // while the tensor cores run S5
+        const PairSetup next = s_next;
+        if (next.p < npairs && next.ok) gather(next);    // X is free: the pending epilogue is done
         if (!tc_wait_all(&mbar, phase)) {
-            if (tid == 0 && status) atomicExch(status, 3);
+            failed = true;
             break;
         }
-
-        // ---- the normalized surface (thread v holds column v), its argmax; 16-column chunks of u
-        // alternate between the two warps of a quadrant
-        const float scale = ldexpf(1.0f, eR + 17) / (float(N) * float(N) * norm);
-        float best = -2.0f;
-        int at = INT_MAX;
-        if (32 * quad < M) {
-            const int v = row;
-            const bool vin = v < M;
-            const float *__restrict__ dv = dvs + (sx & 3) + v;
-            float *__restrict__ sv = surf + v;
-            for (int u0 = 16 * half; u0 < NO; u0 += 32) {   // one 16-column chunk of u per TMEM wait
-                uint32_t cr[16];
-                tc::tmem_ld16_nowait(tmem + lane_base + uint32_t(u0), cr);
-                const int nu = M - u0 < 16 ? M - u0 : 16;   // rows u of the chunk inside the surface
-                float rho[16];
-#pragma unroll
-                for (int e = 0; e < 16; ++e) rho[e] = vin && e < nu ? dv[(u0 + e) * BW] : 0.0f;
-                tc::tmem_wait();
-#pragma unroll
-                for (int e = 0; e < 16; ++e) rho[e] *= __uint_as_float(cr[e]) * scale;
-                if (vin) {
-#pragma unroll
-                    for (int e = 0; e < 16; ++e)
-                        if (e < nu) sv[(u0 + e) * M] = rho[e];
-                }
-                if (vin) {
-#pragma unroll
-                    for (int e = 0; e < 16; ++e)   // values <= -2 and NaN never win; ties keep the first u
-                        if (e < nu && rho[e] > best) {
-                            best = rho[e];
-                            at = u0 + e;
-                        }
-                }
-            }
-            at = at == INT_MAX ? INT_MAX : at * M + v;
-        }
-        for (int o = 16; o > 0; o >>= 1) better(best, at, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, at, o));
-        if (lane == 0) {
-            s_best[warp] = best;
-            s_at[warp] = at;
-        }
-        tc::fence_before_sync();
-        __syncthreads();
-        if (a.surface)
-            for (int i = tid; i < M * M; i += NT) a.surface[q * M * M + i] = surf[i];
-        // every warp: the argmax of the surface, then its rows of the SNR patch's sum of squares
-        best = lane < NT / 32 ? s_best[lane] : -2.0f;
-        at = lane < NT / 32 ? s_at[lane] : INT_MAX;
-        for (int o = 16; o > 0; o >>= 1) better(best, at, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, at, o));
-        double sq = 0.0;
-        if (best > 0) {
-            const int pu = at / M, pv = at % M;
-            if (tid < 9 && pu > 0 && pu < M - 1 && pv > 0 && pv < M - 1)
-                s_fit[tid] = surf[(pu + tid / 3 - 1) * M + pv + tid % 3 - 1];   // the 3 x 3 fit's values
-            else if (tid == 0)
-                s_fit[4] = surf[pu * M + pv];
-            int i0, i1, j0, j1;
-            snr_patch(M, a.stat, pu, pv, i0, i1, j0, j1);
-            for (int i = i0 + warp; i < i1; i += NT / 32)
-                for (int j = j0 + lane; j < j1; j += 32) {
-                    const double c = surf[i * M + j];
-                    sq += c * c;
-                }
-        }
-        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
-        if (lane == 0) s_sq[warp] = sq;
-        pend = {q, at, cur.gy, cur.gx, best > 0, true};
-        __syncthreads();
-        tc::fence_after_sync();
+        prev = {cur.q, cur.f, cur.sy, cur.sx, cur.gy, cur.gx, ldexpf(1.0f, eR + 17) / (float(N) * float(N) * norm), true};
+        cur = next;
     }
-    if (warp == NT / 32 - 1) finish_peak(pend);
+    if (!failed && !epi_flush()) failed = true;
+    if (failed && ctrl && status) atomicExch(status, 3);
+    if (tma_pending) tc::mbar_wait(&tbar, tphase);   // no copy into this CTA's memory may outlive it
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) tc::tmem_dealloc(tmem, G::TMEM_COLS);
