@@ -149,6 +149,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
     __shared__ int s_at[NT / 32];
     __shared__ double s_sq[NT / 32];
     __shared__ float s_fit[9];
+    __shared__ int s_peak[3];   // the pending pair's peak: valid, u, v
     __shared__ PairSetup s_next;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int quad = warp & 3, half = warp >> 2;
@@ -358,6 +359,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
     };
     // the surface's argmax (the first in raster order if equal), then the SNR patch's sum of squares
     // and the 3 x 3 fit's values, read back from TMEM with the same arithmetic
+    // (the compute warps only, with their own barrier: the control thread may still be issuing)
     auto epi_peak = [&]() {
         float best = e_best;
         int at = e_at;
@@ -366,15 +368,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
             s_best[warp] = best;
             s_at[warp] = at;
         }
-        __syncthreads();
-        best = lane < NT / 32 ? s_best[lane] : -2.0f;
-        at = lane < NT / 32 ? s_at[lane] : INT_MAX;
+        asm volatile("bar.sync 1, %0;" ::"n"(32 * kTcCompute) : "memory");
+        best = lane < kTcCompute ? s_best[lane] : -2.0f;
+        at = lane < kTcCompute ? s_at[lane] : INT_MAX;
         for (int o = 16; o > 0; o >>= 1) better(best, at, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, at, o));
         e_valid = best > 0;
         double sq = 0.0;
         if (e_valid) {
             e_pu = at / M;
             e_pv = at % M;
+        }
+        if (tid == 0) {   // for the control thread's solve
+            s_peak[0] = e_valid;
+            s_peak[1] = e_pu;
+            s_peak[2] = e_pv;
+        }
+        if (e_valid) {
             int i0, i1, j0, j1;
             snr_patch(M, a.stat, e_pu, e_pv, i0, i1, j0, j1);
             // the warp pair of a quadrant takes alternate 16-row chunks of u from i0
@@ -406,6 +415,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
     };
     // the FP64 peak solve and the outputs (one thread), from s_fit and s_sq
     auto epi_finish = [&]() {
+        e_valid = s_peak[0] != 0;
+        e_pu = s_peak[1];
+        e_pv = s_peak[2];
         if (!e_valid) {
             invalid_outputs(prev.q, a.offset, a.peak, a.snr, a.cov);
             return;
@@ -413,7 +425,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
         int i0, i1, j0, j1;
         snr_patch(M, a.stat, e_pu, e_pv, i0, i1, j0, j1);
         double sum = 0.0;
-        for (int w = 0; w < NT / 32; ++w) sum += s_sq[w];
+        for (int w = 0; w < kTcCompute; ++w) sum += s_sq[w];
         peak_outputs(s_fit + 4, 3, M, e_pu, e_pv, R, prev.gy, prev.gx, W * W, sum, (i1 - i0) * (j1 - j0), prev.q,
                      a.offset, a.peak, a.snr, a.cov);
     };
@@ -423,7 +435,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
         if (!prev.live) return true;
         epi_fetch();
         const bool ok = epi_normalize();
-        epi_peak();
+        if (compute) epi_peak();
         __syncthreads();
         if (ctrl) epi_finish();
         prev.live = false;
@@ -582,7 +594,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
             }
             tc::mma_commit(&mbar);
         }
-        if (prev.live) epi_peak();   // while the tensor cores run S4
+        if (prev.live && compute) epi_peak();   // while the tensor cores run S4
         if (!tc_wait_all(&mbar, phase)) {
             failed = true;
             break;
