@@ -475,6 +475,56 @@ def run_stream(args):
     }))
 
 
+def run_diff(args):
+    """
+    The differentiable path: 256 x 256 float frames moved by continuous shifts U[-3, 3] (41 moved
+    frames x 25 windows = 1025 windows), window 64, search 8, skip 32. value: the continuous
+    refinement (slipcam_b200.diff.DiffCorrelator.refine, 8 Newton steps, each a forward pass and an
+    adjoint) in windows/s; also one forward + backward of the surfaces (autograd, frames and shift)
+    and the refinement's error against the true shifts. One GPU, CUDA events.
+    """
+    import torch
+    from slipcam_b200 import diff, framecor, synth
+    frames, shifts = synth.shifts_f32(n=42)
+    down, across = framecor.window_grid(256, 256, 64, 8, 32)
+    dc = diff.DiffCorrelator(256, 256, down, across, window=64, search=8)
+    dc.set_reference(torch.as_tensor(frames[0]))
+    f = torch.as_tensor(frames[1:]).cuda()
+    nwin = len(down) * len(across) * f.shape[0]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(args.warmup):
+        r = dc.refine(f, iters=8)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        r = dc.refine(f, iters=8)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    err = np.abs(r['offsets'].cpu().numpy() - shifts[1:, None, None, :]).max(-1)
+    fr = f.clone().requires_grad_(True)
+    sh = torch.full((f.shape[0], len(down), len(across), 2), 0.25, device='cuda', requires_grad=True)
+    for _ in range(args.warmup):
+        (dc.surface(fr, sh) ** 2).sum().backward()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        (dc.surface(fr, sh) ** 2).sum().backward()
+    e1.record()
+    torch.cuda.synchronize()
+    fb_ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps({
+        'metric': 'windows/s, continuous sub-pixel refinement (8 Newton steps: forward + adjoint)',
+        'value': nwin / (ms / 1e3), 'unit': 'windows/s', 'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
+        'data': 'synthetic',
+        'config': {'workload': '41 float 256 x 256 frames moved by U[-3, 3] px, window 64, search 8, skip 32 '
+                               f'({nwin} windows)', 'iterations': 8},
+        'refine_error_px': {'max': float(err.max()), 'median': float(np.median(err))},
+        'surface_forward_backward': {'ms': fb_ms, 'windows': nwin, 'grads': 'frames and shift'},
+    }))
+
+
 def main():
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     p.add_argument('--gpus', type=int, default=1)
@@ -487,14 +537,17 @@ def main():
     p.add_argument('--video', type=int, default=NFRAMES, help='frames of the synthetic video to render')
     p.add_argument('--batch', type=int, default=BATCH, help='frames per step')
     p.add_argument('--form', default='tc', choices=['fft32', 'tc'], help='the arithmetic of the transforms')
-    p.add_argument('--workload', default='hd', choices=['hd', 'mixed', 'stream'],
-                   help='hd: the 720p headline; mixed: three grids in one group step; stream: 1080p streaming')
+    p.add_argument('--workload', default='hd', choices=['hd', 'mixed', 'stream', 'diff'],
+                   help='hd: the 720p headline; mixed: three grids in one group step; stream: 1080p streaming; '
+                        'diff: the differentiable path')
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.workload == 'mixed' and args.impl != 'reference':
         run_mixed(args)
     elif args.workload == 'stream' and args.impl != 'reference':
         run_stream(args)
+    elif args.workload == 'diff' and args.impl != 'reference':
+        run_diff(args)
     elif args.impl == 'reference':
         run_reference(args)
     else:

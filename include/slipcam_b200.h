@@ -163,6 +163,13 @@ B200_API int b200_group_config(const b200_group *g, int *threads, int *chunk, in
 B200_API int b200_group_set_config(b200_group *g, int threads, int chunk, int costly_first, int per_grid,
                                    int use_graph);
 
+/* auto_slip.periodicity (python/slipcam/auto_slip.py:105-129) for every window of the handle's
+ * grid: surface holds the normalized surfaces of the reference frame correlated with itself
+ * (b200_correlate_device_surfaces with the reference as the one frame), n_windows x (2R+1)^2; out
+ * (n_windows floats, device memory) receives the largest 5 x 5 local maximum outside the
+ * (2 exclude + 1)^2 box around zero shift, 1 for a flat window, 0 if no peak is left. */
+B200_API int b200_periodicity_device(b200_handle *h, const float *surface, int exclude, float *out, void *stream);
+
 /* ---- The differentiable path: float frames, a continuous shift per pair, and the adjoints.
  * No counterpart in the reference (its backends take uint8 frames and give no derivatives); the
  * math follows the same correlation (cxx/cpu.cpp:115-160, cxx/surface.h:30-146) and is stated in

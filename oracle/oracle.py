@@ -177,3 +177,33 @@ def reference_module():
         sys.modules.setdefault('_oracle_ref_framecor', mod)
         _ref_module = mod
     return _ref_module
+
+
+def periodicity(ref, y0, x0, window, search, exclude=5):
+    """
+    TEST INFRASTRUCTURE. The restatement of auto_slip.periodicity (python/slipcam/auto_slip.py:105-129):
+    for each window of the uint8 reference frame, its normalized correlation with its own
+    surroundings (the FP64 direct oracle's surface, the search window around the window itself),
+    the 5 x 5 local maxima of that surface with reflecting borders (scipy.ndimage.maximum_filter's
+    default), without those in the (2 exclude + 1)^2 box around zero shift (the same slice as the
+    reference, negative starts included), and the largest of them; 1 for a flat window (norm below
+    1e-6), 0 if no peak is left.
+    """
+    ref = np.ascontiguousarray(ref, np.uint8)
+    h, w = ref.shape
+    y0, x0 = np.asarray(y0), np.asarray(x0)
+    o = correlate(h, w, y0, x0, ref, ref[None], None, window=window, search=search, mode='f64', surfaces=True)
+    _, norms = reference_windows(h, w, y0, x0, window, ref)
+    norms = np.asarray(norms).reshape(len(y0), len(x0))
+    out = np.ones((len(y0), len(x0)))
+    c = search
+    for i in range(len(y0)):
+        for j in range(len(x0)):
+            if norms[i, j] < 1e-6:
+                continue
+            s = o['surface'][0, i, j].astype(np.float64)
+            local = np.lib.stride_tricks.sliding_window_view(np.pad(s, 2, mode='symmetric'), (5, 5)).max(axis=(-2, -1))
+            peaks = s == local
+            peaks[c - exclude:c + exclude + 1, c - exclude:c + exclude + 1] = False
+            out[i, j] = s[peaks].max() if peaks.any() else 0.0
+    return out

@@ -45,6 +45,7 @@ SIGNATURES = {
     'b200_group_config': (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i),
                                ctypes.POINTER(_i)]),
     'b200_group_set_config': (_i, [_vp, _i, _i, _i, _i, _i]),
+    'b200_periodicity_device': (_i, [_vp, _vp, _i, _vp, _vp]),
     'b200_set_reference_f32_device': (_i, [_vp, _vp, _i, _vp]),
     'b200_diff_forward': (_i, [_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     'b200_diff_backward': (_i, [_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

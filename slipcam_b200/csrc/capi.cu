@@ -25,6 +25,7 @@
 #include "corr_tc.cuh"
 #include "diff.h"
 #include "multi.h"
+#include "periodicity.cuh"
 #include "sat.cuh"
 #include "tc_selftest.cuh"
 
@@ -941,6 +942,20 @@ int b200_tc_selftest(const void *A, const void *B, float *D, int N, int K, int a
     cudaFreeAsync(status, s);
     if (!ok) return B200_ERUNTIME;
     return h ? B200_ETIMEOUT : B200_OK;
+}
+
+int b200_periodicity_device(b200_handle *h, const float *surface, int exclude, float *out, void *stream)
+{
+    return guarded(h, [&] {
+        if (!h->ready) fail(B200_ERUNTIME, "set_reference first");
+        if (!surface || !out) fail(B200_EINVAL, "null input or output");
+        if (exclude < 0) fail(B200_EINVAL, "the exclusion must not be negative");
+        CK(cudaSetDevice(h->device));
+        periodicity_kernel<256><<<unsigned(h->nwin), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+            surface, h->d_norm.p, h->M, h->R, exclude, out);
+        CK(cudaGetLastError());
+        h->launches += 1;
+    });
 }
 
 int b200_set_reference_f32_device(b200_handle *h, const float *frame, int pitch, void *stream)

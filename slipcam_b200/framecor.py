@@ -257,6 +257,31 @@ def sat(frames):
     return s32.to(torch.int64) & 0xFFFFFFFF, s64
 
 
+def periodicity(ref, y0, x0, window, search, exclude=5):
+    """
+    auto_slip.periodicity (python/slipcam/auto_slip.py:105-129) on the b200 backend: the second peak
+    of the normalized correlation of each window with its own surroundings in the reference frame
+    (1 for a periodic or flat texture, small for a unique one), as a float64 (len(y0), len(x0))
+    array. The surfaces are the b200 correlation of the frame with itself (FP32); the peak search
+    runs on the GPU. ref: uint8 (height, width), numpy or a CUDA tensor.
+    """
+    import torch
+    f = torch.as_tensor(np.asarray(ref) if not _is_torch(ref) else ref)
+    if f.dim() != 2:
+        raise ValueError('framecor: the reference frame must be height x width')
+    f = f.to(torch.uint8).cuda().contiguous()
+    h, w = f.shape
+    cor = Correlator(h, w, y0, x0, window=window, search=search, backend='b200')
+    cor.set_reference(f)
+    surf = cor.correlate(f[None], surfaces=True)['surface']
+    ny, nx = cor.shape
+    out = torch.empty(ny * nx, dtype=torch.float32, device=f.device)
+    stream = torch.cuda.current_stream(f.device).cuda_stream
+    rc = _lib.lib().b200_periodicity_device(cor._h, surf.data_ptr(), int(exclude), out.data_ptr(), stream)
+    _lib.raise_for(rc, cor._h)
+    return out.view(ny, nx).cpu().numpy().astype(np.float64)
+
+
 class MultiCorrelator:
     """
     Several window grids (window sizes, search ranges, grids) of one video correlated together:
