@@ -170,6 +170,26 @@ B200_API int b200_group_set_config(b200_group *g, int threads, int chunk, int co
  * (2 exclude + 1)^2 box around zero shift, 1 for a flat window, 0 if no peak is left. */
 B200_API int b200_periodicity_device(b200_handle *h, const float *surface, int exclude, float *out, void *stream);
 
+/* ---- The frame scans of auto_slip (python/slipcam/auto_slip.py:56-94), on device memory. Frames
+ * are uint8, rows `pitch` bytes apart, frames pitch * height bytes apart.
+ * b200_frame_diff_device: out[k] = the mean |frames[k + 1] - frames[k]| over the pixels, k < n - 1
+ * (frame_differences, auto_slip.py:56-63; the sums exact); sums: n - 1 caller-owned uint64. */
+B200_API int b200_frame_diff_device(const uint8_t *frames, int n, int height, int width, int pitch, float *out,
+                                    uint64_t *sums, void *stream);
+/* out (height x width float32): per pixel, the median over nchunks consecutive chunks of `chunk`
+ * frames of the population standard deviation within a chunk (text_mask, auto_slip.py:87-90). */
+B200_API int b200_chunk_std_median_device(const uint8_t *frames, int nchunks, int chunk, int height, int width,
+                                          int pitch, float *out, void *stream);
+/* out (height x width float32): hypot of the two Sobel derivatives of a frame, borders reflected
+ * (scipy.ndimage.sobel, auto_slip.py:91). */
+B200_API int b200_sobel_device(const uint8_t *frame, int height, int width, int pitch, float *out, void *stream);
+/* The text mask from the edge magnitude and the temporal deviation (auto_slip.py:92-94): edge > thr
+ * and sd < max_std, `dilate` steps of the 3 x 3 cross dilation, then the holes (background not
+ * 4-connected to the border) filled. mask: height x width bytes (0 / 1); scratch: 2 x height x
+ * width bytes; flag: one int. Synchronous on `stream` (the fill runs until nothing changes). */
+B200_API int b200_text_mask_device(const float *edge, const float *sd, int height, int width, float thr, float max_std,
+                                   int dilate, uint8_t *mask, uint8_t *scratch, int *flag, void *stream);
+
 /* ---- The differentiable path: float frames, a continuous shift per pair, and the adjoints.
  * No counterpart in the reference (its backends take uint8 frames and give no derivatives); the
  * math follows the same correlation (cxx/cpu.cpp:115-160, cxx/surface.h:30-146) and is stated in

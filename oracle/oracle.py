@@ -207,3 +207,59 @@ def periodicity(ref, y0, x0, window, search, exclude=5):
             peaks[c - exclude:c + exclude + 1, c - exclude:c + exclude + 1] = False
             out[i, j] = s[peaks].max() if peaks.any() else 0.0
     return out
+
+
+def frame_differences(frames, chunk=50):
+    """
+    TEST INFRASTRUCTURE. The restatement of auto_slip.frame_differences (auto_slip.py:56-63): the
+    mean absolute difference of consecutive uint8 frames, from exact integer sums (float32 result).
+    """
+    f = np.asarray(frames)
+    out = np.empty(len(f) - 1, np.float32)
+    for k in range(len(f) - 1):
+        s = np.abs(f[k + 1].astype(np.int64) - f[k].astype(np.int64)).sum()
+        out[k] = np.float32(s / f[k].size)
+    return out
+
+
+def _sobel_magnitude(img):
+    """hypot of the two Sobel derivatives of a float32 image, borders reflected (half-sample)"""
+    p = np.pad(img.astype(np.float64), 1, mode='symmetric')
+    rows = lambda d: p[1 + d:p.shape[0] - 1 + d]
+    cols = lambda a, d: a[:, 1 + d:a.shape[1] - 1 + d]
+    g0 = cols(rows(1) - rows(-1), -1) + 2 * cols(rows(1) - rows(-1), 0) + cols(rows(1) - rows(-1), 1)
+    dc = cols(p, 1) - cols(p, -1)
+    g1 = dc[:-2] + 2 * dc[1:-1] + dc[2:]
+    return np.hypot(g0.astype(np.float32), g1.astype(np.float32))
+
+
+def text_mask(frames, start, nframes=150, chunk=10, edge_percentile=90, max_std=1.5, dilate=4):
+    """
+    TEST INFRASTRUCTURE. The restatement of auto_slip.text_mask (auto_slip.py:81-94): the per-pixel
+    population standard deviation of each chunk of frames (exact integer sums), its median over the
+    chunks; the Sobel magnitude of frame start; strong (above the percentile) and steady (below
+    max_std) pixels, dilated `dilate` times by the 3 x 3 cross, then every background region that
+    does not touch the border (4-connected) filled.
+    """
+    from scipy import ndimage
+    f = np.asarray(frames)
+    stds = []
+    for a in range(start, min(start + nframes, len(f)) - chunk + 1, chunk):
+        x = f[a:a + chunk].astype(np.int64)
+        s1, s2 = x.sum(0), (x * x).sum(0)
+        var = (chunk * s2 - s1 * s1) / float(chunk * chunk)
+        stds.append(np.sqrt(np.maximum(var, 0)).astype(np.float32))
+    sd = np.median(np.stack(stds), axis=0)
+    edge = _sobel_magnitude(f[start].astype(np.float32))
+    m = (edge > np.percentile(edge, edge_percentile)) & (sd < max_std)
+    for _ in range(dilate):
+        g = m.copy()
+        g[1:] |= m[:-1]
+        g[:-1] |= m[1:]
+        g[:, 1:] |= m[:, :-1]
+        g[:, :-1] |= m[:, 1:]
+        m = g
+    labels, _ = ndimage.label(~m)   # 4-connected background regions
+    border = np.unique(np.concatenate([labels[0], labels[-1], labels[:, 0], labels[:, -1]]))
+    outside = np.isin(labels, border[border > 0])
+    return ~outside

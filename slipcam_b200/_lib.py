@@ -46,6 +46,10 @@ SIGNATURES = {
                                ctypes.POINTER(_i)]),
     'b200_group_set_config': (_i, [_vp, _i, _i, _i, _i, _i]),
     'b200_periodicity_device': (_i, [_vp, _vp, _i, _vp, _vp]),
+    'b200_frame_diff_device': (_i, [_vp, _i, _i, _i, _i, _vp, _vp, _vp]),
+    'b200_chunk_std_median_device': (_i, [_vp, _i, _i, _i, _i, _i, _vp, _vp]),
+    'b200_sobel_device': (_i, [_vp, _i, _i, _i, _vp, _vp]),
+    'b200_text_mask_device': (_i, [_vp, _vp, _i, _i, ctypes.c_float, ctypes.c_float, _i, _vp, _vp, _vp, _vp]),
     'b200_set_reference_f32_device': (_i, [_vp, _vp, _i, _vp]),
     'b200_diff_forward': (_i, [_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     'b200_diff_backward': (_i, [_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

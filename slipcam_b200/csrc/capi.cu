@@ -26,6 +26,7 @@
 #include "diff.h"
 #include "multi.h"
 #include "periodicity.cuh"
+#include "scans.cuh"
 #include "sat.cuh"
 #include "tc_selftest.cuh"
 
@@ -942,6 +943,76 @@ int b200_tc_selftest(const void *A, const void *B, float *D, int N, int K, int a
     cudaFreeAsync(status, s);
     if (!ok) return B200_ERUNTIME;
     return h ? B200_ETIMEOUT : B200_OK;
+}
+
+namespace {
+__global__ void frame_diff_means_kernel(const unsigned long long *sums, int n, double npix, float *out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) out[k] = float(double(sums[k]) / npix);
+}
+unsigned blocks_for(int64_t n, int per = 256) { return unsigned((n + per - 1) / per); }
+}   // namespace
+
+int b200_frame_diff_device(const uint8_t *frames, int n, int height, int width, int pitch, float *out, uint64_t *sums,
+                           void *stream)
+{
+    if (n < 0 || height <= 0 || width <= 0 || pitch < width || (n > 1 && (!frames || !out || !sums))) return B200_EINVAL;
+    if (n < 2) return B200_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned long long *us = reinterpret_cast<unsigned long long *>(sums);
+    if (cudaMemsetAsync(us, 0, size_t(n - 1) * sizeof(uint64_t), s) != cudaSuccess) return B200_ERUNTIME;
+    const unsigned bands = unsigned(std::min(height, 64));
+    frame_diff_kernel<<<dim3(bands, unsigned(n - 1)), 256, 0, s>>>(frames, int64_t(pitch) * height, pitch, height, width, us);
+    frame_diff_means_kernel<<<blocks_for(n - 1), 256, 0, s>>>(us, n - 1, double(height) * width, out);
+    return cudaGetLastError() == cudaSuccess ? B200_OK : B200_ERUNTIME;
+}
+
+int b200_chunk_std_median_device(const uint8_t *frames, int nchunks, int chunk, int height, int width, int pitch,
+                                 float *out, void *stream)
+{
+    if (nchunks < 1 || nchunks > kScanMaxChunks || chunk < 1 || height <= 0 || width <= 0 || pitch < width || !frames || !out)
+        return B200_EINVAL;
+    chunk_std_median_kernel<<<blocks_for(int64_t(height) * width), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        frames, int64_t(pitch) * height, pitch, height, width, chunk, nchunks, out);
+    return cudaGetLastError() == cudaSuccess ? B200_OK : B200_ERUNTIME;
+}
+
+int b200_sobel_device(const uint8_t *frame, int height, int width, int pitch, float *out, void *stream)
+{
+    if (height <= 0 || width <= 0 || pitch < width || !frame || !out) return B200_EINVAL;
+    sobel_kernel<<<blocks_for(int64_t(height) * width), 256, 0, static_cast<cudaStream_t>(stream)>>>(frame, pitch, height,
+                                                                                                      width, out);
+    return cudaGetLastError() == cudaSuccess ? B200_OK : B200_ERUNTIME;
+}
+
+int b200_text_mask_device(const float *edge, const float *sd, int height, int width, float thr, float max_std, int dilate,
+                          uint8_t *mask, uint8_t *scratch, int *flag, void *stream)
+{
+    if (height <= 0 || width <= 0 || dilate < 0 || !edge || !sd || !mask || !scratch || !flag) return B200_EINVAL;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t n = int64_t(height) * width;
+    const unsigned nb = blocks_for(n);
+    uint8_t *a = scratch, *b = scratch + n;
+    text_seed_kernel<<<nb, 256, 0, s>>>(edge, sd, n, thr, max_std, a);
+    for (int i = 0; i < dilate; ++i) {
+        dilate_kernel<<<nb, 256, 0, s>>>(a, b, height, width);
+        std::swap(a, b);
+    }
+    // the background reached from the border; a step spreads it one pixel, so check every 32
+    outside_init_kernel<<<nb, 256, 0, s>>>(a, b, height, width);
+    for (int64_t done = 0; done < n; done += 32) {
+        if (cudaMemsetAsync(flag, 0, sizeof(int), s) != cudaSuccess) return B200_ERUNTIME;
+        for (int i = 0; i < 32; ++i) outside_step_kernel<<<nb, 256, 0, s>>>(a, b, height, width, flag);
+        int changed = 0;
+        if (cudaMemcpyAsync(&changed, flag, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return B200_ERUNTIME;
+        if (!changed) break;
+    }
+    fill_kernel<<<nb, 256, 0, s>>>(b, mask, n);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return B200_ERUNTIME;
+    return B200_OK;
 }
 
 int b200_periodicity_device(b200_handle *h, const float *surface, int exclude, float *out, void *stream)

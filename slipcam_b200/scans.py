@@ -1,0 +1,85 @@
+"""
+The frame scans of auto_slip (python/slipcam/auto_slip.py:56-94) on the b200 backend: the mean
+absolute difference of consecutive frames and the burned-in text mask, as CUDA passes over the
+uint8 frames (csrc/scans.cuh). Same arguments and results as the reference functions; frames are a
+numpy array (memory-mapped or not; copied to the GPU in chunks) or a CUDA tensor.
+"""
+
+import numpy as np
+
+from . import _lib
+
+
+def _check(rc):
+    if rc != _lib.OK:
+        raise (ValueError if rc == _lib.EINVAL else RuntimeError)(f'framecor: scan failed ({rc})')
+
+
+def _device(frames, a, b):
+    """frames[a:b] as a contiguous uint8 CUDA tensor"""
+    import torch
+    if isinstance(frames, torch.Tensor):
+        return frames[a:b].to(device='cuda', dtype=torch.uint8).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(frames[a:b], np.uint8)).cuda()
+
+
+def frame_differences(frames, chunk=50):
+    """The mean absolute difference of consecutive frames, float32 (n - 1,) (auto_slip.py:56-63)"""
+    import torch
+    n = len(frames)
+    if n < 2:
+        return np.empty(0, np.float32)
+    h, w = frames.shape[1:]
+    out = torch.empty(n - 1, dtype=torch.float32, device='cuda')
+    sums = torch.empty(n - 1, dtype=torch.int64, device='cuda')
+    stream = torch.cuda.current_stream().cuda_stream
+    for a in range(0, n - 1, chunk):   # chunk + 1 frames: the pairs (a, a + 1) .. (b - 2, b - 1)
+        b = min(a + chunk + 1, n)
+        f = _device(frames, a, b)
+        _check(_lib.lib().b200_frame_diff_device(f.data_ptr(), b - a, h, w, w, out[a:].data_ptr(), sums[a:].data_ptr(),
+                                                 stream))
+    return out.cpu().numpy()
+
+
+def _percentile_like_numpy(x, q):
+    """numpy.percentile(x, q) of a float32 CUDA tensor (the 'linear' method and numpy's lerp, float32
+    result), from its two order statistics"""
+    import torch
+    v = x.flatten()
+    n = v.numel()
+    idx = q / 100.0 * (n - 1)
+    lo = int(np.floor(idx))
+    hi = min(lo + 1, n - 1)
+    t = idx - lo
+    a = np.float32(torch.kthvalue(v, lo + 1).values.item())
+    b = np.float32(torch.kthvalue(v, hi + 1).values.item())
+    diff = np.float32(b - a)
+    r = a + diff * t if t < 0.5 else b - diff * (1 - t)
+    return np.float32(r)
+
+
+def text_mask(frames, start, nframes=150, chunk=10, edge_percentile=90, max_std=1.5, dilate=4):
+    """The pixels of burned-in text, bool (height, width) (auto_slip.py:81-94): strong edges of the
+    frame start (above the edge_percentile of its Sobel magnitude) whose values hardly change (the
+    median over chunks of the temporal standard deviation below max_std), dilated and with the
+    regions they enclose filled."""
+    import torch
+    n = len(frames)
+    h, w = frames.shape[1:]
+    starts = list(range(start, min(start + nframes, n) - chunk + 1, chunk))
+    if not starts:
+        raise ValueError('framecor: no complete chunk of frames for the text mask')
+    stream = torch.cuda.current_stream().cuda_stream
+    f = _device(frames, starts[0], starts[-1] + chunk)
+    sd = torch.empty((h, w), dtype=torch.float32, device='cuda')
+    _check(_lib.lib().b200_chunk_std_median_device(f.data_ptr(), len(starts), chunk, h, w, w, sd.data_ptr(), stream))
+    ref = _device(frames, start, start + 1)
+    edge = torch.empty((h, w), dtype=torch.float32, device='cuda')
+    _check(_lib.lib().b200_sobel_device(ref.data_ptr(), h, w, w, edge.data_ptr(), stream))
+    thr = _percentile_like_numpy(edge, edge_percentile)
+    mask = torch.empty((h, w), dtype=torch.uint8, device='cuda')
+    scratch = torch.empty(2 * h * w, dtype=torch.uint8, device='cuda')
+    flag = torch.empty(1, dtype=torch.int32, device='cuda')
+    _check(_lib.lib().b200_text_mask_device(edge.data_ptr(), sd.data_ptr(), h, w, float(thr), float(max_std), int(dilate),
+                                            mask.data_ptr(), scratch.data_ptr(), flag.data_ptr(), stream))
+    return mask.cpu().numpy().astype(bool)
