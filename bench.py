@@ -525,6 +525,63 @@ def run_diff(args):
     }))
 
 
+def run_stabilize(args):
+    """
+    Coarse similarity tracking (stabilize.coarse_track, the reference's defaults: 96-px templates 96
+    px apart, +-32 px search, min_peak 0.5): a 720p camera video (a random walk of 2 px, 1e-3 rad and
+    1e-3 scale per frame, two burned-in text boxes) tracked from frame 0. A step tracks the whole
+    video; the frames are sequential (each is searched around the previous one's prediction), so a
+    frame is a latency-bound chain of three launches. value: device-resident frames on prepared
+    templates (CUDA events); e2e: coarse_track from a host array, templates included; cpu_baseline:
+    the oracle's restatement of the reference (numpy FFT, one thread) on a few frames. One GPU.
+    """
+    import torch
+    from oracle import oracle
+    from slipcam_b200 import stabilize, synth
+    n = args.video if args.video != NFRAMES else 200
+    text_boxes = ((900, 24, 1240, 68), (40, 650, 630, 700))
+    frames, truth, text = synth.camera(n, 720, 1280, ref=0, seed=11, walk=(2.0, 2.0, 0.001, 0.001), text=text_boxes,
+                                       device='cuda')
+    host = frames.cpu().numpy()
+    tr = stabilize.CoarseTracker(frames[0], text)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(args.warmup):
+        p, u, c = tr.run(frames, 0)
+    torch.cuda.synchronize()
+    steps = max(1, min(args.steps, 10))
+    e0.record()
+    for _ in range(steps):
+        p, u, c = tr.run(frames, 0)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    t = time.perf_counter()
+    pe, ue, _ = stabilize.coarse_track(host, 0, text)
+    e2e_s = time.perf_counter() - t
+    cpu_frames = 4
+    t = time.perf_counter()
+    po, uo, _ = oracle.coarse_track(host[:cpu_frames + 1], 0, text)
+    cpu_s = time.perf_counter() - t
+    err = np.abs(p - truth)
+    print(json.dumps({
+        'metric': 'frames/s, coarse similarity tracking of a 720p video (stabilize.coarse_track defaults)',
+        'value': (n - 1) / (ms / 1e3), 'unit': 'frames/s', 'n_gpus': 1, 'steps': steps, 'warmup': args.warmup,
+        'ms_per_step': ms, 'us_per_frame': ms * 1e3 / (n - 1), 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f32 correlation, f64 fit', 'data': 'synthetic',
+        'config': {'workload': f'720p camera video, {n} frames, window 96, step 96, search 32 ({tr.nwin} templates, '
+                               f'{c} in use)', 'form': 'fft32'},
+        'e2e': {'value': (n - 1) / e2e_s, 'unit': 'frames/s', 'h2d_bytes_per_step': (n - 1) * 720 * 1280,
+                'd2h_bytes_per_step': (n - 1) * 36, 'path': 'stabilize.coarse_track over a host array'},
+        'gpu_launches': 3 * (n - 1) + 3 * ((n - 1 + 31) // 32),
+        'cpu_baseline': {'value': cpu_frames / cpu_s, 'unit': 'frames/s', 'cores': 1, 'kind': 'port',
+                         'sample': f'{cpu_frames} frames of the same video ({cpu_s:.1f} s)'},
+        'agreement': {'vs_oracle_max_px': float(np.abs(po[1:] - p[1:cpu_frames + 1])[:, :2].max()),
+                      'used_equal': bool(np.array_equal(uo[1:], u[1:cpu_frames + 1])),
+                      'host_equals_device': bool(np.array_equal(pe, p))},
+        'error_vs_truth': {'shift_px': float(err[:, :2].max()), 'rotation_scale': float(err[:, 2:].max())},
+    }))
+
+
 def main():
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     p.add_argument('--gpus', type=int, default=1)
@@ -537,9 +594,9 @@ def main():
     p.add_argument('--video', type=int, default=NFRAMES, help='frames of the synthetic video to render')
     p.add_argument('--batch', type=int, default=BATCH, help='frames per step')
     p.add_argument('--form', default='tc', choices=['fft32', 'tc'], help='the arithmetic of the transforms')
-    p.add_argument('--workload', default='hd', choices=['hd', 'mixed', 'stream', 'diff'],
+    p.add_argument('--workload', default='hd', choices=['hd', 'mixed', 'stream', 'diff', 'stabilize'],
                    help='hd: the 720p headline; mixed: three grids in one group step; stream: 1080p streaming; '
-                        'diff: the differentiable path')
+                        'diff: the differentiable path; stabilize: coarse similarity tracking')
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.workload == 'mixed' and args.impl != 'reference':
@@ -548,6 +605,8 @@ def main():
         run_stream(args)
     elif args.workload == 'diff' and args.impl != 'reference':
         run_diff(args)
+    elif args.workload == 'stabilize' and args.impl != 'reference':
+        run_stabilize(args)
     elif args.impl == 'reference':
         run_reference(args)
     else:

@@ -170,6 +170,47 @@ B200_API int b200_group_set_config(b200_group *g, int threads, int chunk, int co
  * (2 exclude + 1)^2 box around zero shift, 1 for a flat window, 0 if no peak is left. */
 B200_API int b200_periodicity_device(b200_handle *h, const float *surface, int exclude, float *out, void *stream);
 
+/* ---- The coarse similarity tracking of stabilize (python/slipcam/stabilize.py:22-96), on device
+ * memory, stream-ordered on `stream`. One frame is: b200_correlate_device_surfaces of the frame
+ * with the handle of the grid of templates (window, search as in coarse_track; gross per window),
+ * b200_ncc_peaks_device on its surfaces, then b200_coarse_fit_device, which also writes the gross
+ * offsets of the next frame: the frames follow one another without a host round trip.
+ *
+ * b200_ncc_peaks_device: the peak of ncc_peak (stabilize.py:22-44) in each of n surfaces of M x M
+ * floats: out (n x 3 doubles) receives (dy, dx) of the largest value relative to the surface
+ * centre, refined by a parabola per axis, and the value. */
+B200_API int b200_ncc_peaks_device(const float *surface, int n, int M, double *out, void *stream);
+
+/* The most windows of one grid of b200_coarse_fit_device */
+#define B200_COARSE_MAX_WINDOWS 2048
+
+/* The rest of one frame of coarse_track (stabilize.py:80-95) with slip_series.fit_camera
+ * (python/slipcam/slip_series.py:49-72), for the grid of ny x nx windows centred at (yc[i], xc[j])
+ * in frames of height x width: peaks (ny nx x 3, from b200_ncc_peaks_device), gross (ny nx x 2
+ * int32, the frame's gross offsets: the rounded predicted centres minus the grid's; overwritten
+ * with the next frame's), keep (ny nx bytes: the window is used). prev (4 doubles): the transform
+ * (p, q, a, s) the frame was predicted from, replaced by the frame's when it has a fit. params
+ * (4 doubles) receives the frame's transform and used (1 int32) the number of windows of its fit
+ * (0 when there is none: params = prev). Zero prev and gross to start a pass from the reference. */
+B200_API int b200_coarse_fit_device(const double *peaks, int32_t *gross, const uint8_t *keep, const int32_t *yc,
+                                    const int32_t *xc, int ny, int nx, int height, int width, int window,
+                                    int search, double min_peak, double *prev, double *params, int32_t *used,
+                                    void *stream);
+
+/* coarse_track's frame loop (stabilize.py:76-95) on the handle h of the grid of templates
+ * (created with the grid's first rows and columns, window and search as coarse_track places them;
+ * the window even; its reference frame set): n frames (device memory, rows `pitch` bytes apart,
+ * frames pitch * height bytes apart) in the order they are tracked, each searched around the
+ * positions predicted by the previous one, its transform written to params (n x 4 doubles) and the
+ * windows of its fit to used (n int32). keep (windows bytes): the templates in use. gross
+ * (windows x 2 int32) and prev (4 doubles) carry the prediction from call to call; reset != 0 zeroes
+ * them first (the start of a pass from the reference). Per group of frames the tables in one batch,
+ * then per frame three launches: the FP32 correlation (whatever the handle's form), the peaks, the
+ * fit. The handle keeps one frame's surfaces and peaks (allocated by the first call). */
+B200_API int b200_coarse_track_device(b200_handle *h, const uint8_t *frames, int n, int pitch, const uint8_t *keep,
+                                      double min_peak, int reset, int32_t *gross, double *prev, double *params,
+                                      int32_t *used, void *stream);
+
 /* ---- The frame scans of auto_slip (python/slipcam/auto_slip.py:56-94), on device memory. Frames
  * are uint8, rows `pitch` bytes apart, frames pitch * height bytes apart.
  * b200_frame_diff_device: out[k] = the mean |frames[k + 1] - frames[k]| over the pixels, k < n - 1

@@ -263,3 +263,116 @@ def text_mask(frames, start, nframes=150, chunk=10, edge_percentile=90, max_std=
     border = np.unique(np.concatenate([labels[0], labels[-1], labels[:, 0], labels[:, -1]]))
     outside = np.isin(labels, border[border > 0])
     return ~outside
+
+
+def ncc_peak(template, search):
+    """
+    TEST INFRASTRUCTURE. The restatement of stabilize.ncc_peak (python/slipcam/stabilize.py:22-44):
+    the normalized correlation of the zero-mean template at every placement inside search (the
+    products by FFT in float64, the box sums of the search exactly by cumulative sums; the variance
+    floored at 1e-6), its largest value (the first if equal), a parabola per axis through it and its
+    neighbours (no refinement at the edge or for a denominator below 1e-12), as (dy, dx) from the
+    centre of the placements, and the value. A flat template gives (NaN, NaN, 0).
+    """
+    t = np.asarray(template, np.float64)
+    s = np.asarray(search, np.float64)
+    t0 = t - t.mean()
+    tn = np.sqrt((t0 * t0).sum())
+    if tn < 1e-6:
+        return np.nan, np.nan, 0.0
+    th, tw = t.shape
+    H, W = s.shape
+    num = np.fft.irfft2(np.fft.rfft2(s) * np.conj(np.fft.rfft2(t0, s=(H, W))), s=(H, W))[:H - th + 1, :W - tw + 1]
+
+    def box(a):
+        c = np.zeros((H + 1, W + 1))
+        c[1:, 1:] = a.cumsum(0).cumsum(1)
+        return c[th:, tw:] - c[:-th, tw:] - c[th:, :-tw] + c[:-th, :-tw]
+    ssum, ssq = box(s), box(s * s)
+    ncc = num / (np.sqrt(np.maximum(ssq - ssum * ssum / t.size, 1e-6)) * tn)
+    i, j = np.unravel_index(int(np.argmax(ncc)), ncc.shape)
+
+    def vertex(c, m, p):
+        den = m - 2 * c + p
+        return 0.0 if abs(den) < 1e-12 else 0.5 * (m - p) / den
+    di = vertex(ncc[i, j], ncc[i - 1, j], ncc[i + 1, j]) if 0 < i < ncc.shape[0] - 1 else 0.0
+    dj = vertex(ncc[i, j], ncc[i, j - 1], ncc[i, j + 1]) if 0 < j < ncc.shape[1] - 1 else 0.0
+    return i + di - (ncc.shape[0] - 1) / 2, j + dj - (ncc.shape[1] - 1) / 2, ncc[i, j]
+
+
+def fit_camera(dx, dy, x, y, iterations=3):
+    """
+    TEST INFRASTRUCTURE. The restatement of slip_series.fit_camera (python/slipcam/slip_series.py:
+    49-72), similarity model: least squares of dx = p - a y + s x, dy = q + a x + s y over the points
+    with both offsets finite, `iterations` times, each time dropping the points whose residual, in
+    either component, is not below max(3 x 1.4826 x the median absolute deviation of the residuals
+    in use, 0.3); NaN and 0 when fewer than 4 points are left at the start of a round. Returns the
+    last fit and the number of points left after the last round.
+    """
+    dx, dy, x, y = (np.asarray(v, np.float64) for v in (dx, dy, x, y))
+    use = np.isfinite(dx) & np.isfinite(dy)
+    m = np.full(4, np.nan)
+    for _ in range(iterations):
+        if use.sum() < 4:
+            return np.full(4, np.nan), 0
+        k = np.flatnonzero(use)
+        G = np.vstack([np.column_stack([np.ones(len(k)), np.zeros(len(k)), -y[k], x[k]]),
+                       np.column_stack([np.zeros(len(k)), np.ones(len(k)), x[k], y[k]])])
+        m = np.linalg.lstsq(G, np.concatenate([dx[k], dy[k]]), rcond=None)[0]
+        rx = dx[k] - (m[0] - m[2] * y[k] + m[3] * x[k])
+        ry = dy[k] - (m[1] + m[2] * x[k] + m[3] * y[k])
+        r = np.concatenate([rx, ry])
+        thr = max(3 * 1.4826 * np.median(np.abs(r - np.median(r))), 0.3)
+        use[k] = (np.abs(rx) < thr) & (np.abs(ry) < thr)
+    return m, int(use.sum())
+
+
+def coarse_track(frames, ref, text, window=96, step=96, search=32, min_peak=0.5, start=0):
+    """
+    TEST INFRASTRUCTURE. The restatement of stabilize.coarse_track (python/slipcam/stabilize.py:
+    54-96): the grid of window x window templates of the reference frame centred `search + half`
+    pixels or more inside it, `step` apart, without those that touch the text mask or whose
+    standard deviation is 2 or less; each frame, forward from ref then backward to start, searched
+    +-search pixels around each template's position predicted by the previous frame's similarity
+    transform (rounded half to even), the peaks of at least min_peak fitted by fit_camera. Returns
+    (frames x 4 transforms, windows per fit, templates in use).
+    """
+    f = np.asarray(frames)
+    n, h, w = f.shape
+    half = window // 2
+    ys = np.arange(search + half, h - search - half, step)
+    xs = np.arange(search + half, w - search - half, step)
+    cy, cx = (v.ravel() for v in np.meshgrid(ys, xs, indexing='ij'))
+    refimg = f[ref].astype(np.float64)
+    text = np.asarray(text, bool)
+    sel = [not text[a - half:a + half, b - half:b + half].any() and refimg[a - half:a + half, b - half:b + half].std() > 2
+           for a, b in zip(cy, cx)]
+    sel = np.asarray(sel, bool)
+    cy, cx = cy[sel], cx[sel]
+    X, Y = cx - w / 2, cy - h / 2
+    L = window + 2 * search
+    params = np.full((n, 4), np.nan)
+    used = np.zeros(n, int)
+    params[ref], used[ref] = 0, len(cx)
+    for frames_in_order in (range(ref + 1, n), range(ref - 1, start - 1, -1)):
+        prev = np.zeros(4)
+        for k in frames_in_order:
+            img = f[k].astype(np.float64)
+            px = X + prev[0] - prev[2] * Y + prev[3] * X + w / 2
+            py = Y + prev[1] + prev[2] * X + prev[3] * Y + h / 2
+            dx, dy = np.full(len(cx), np.nan), np.full(len(cx), np.nan)
+            for t in range(len(cx)):
+                top, left = int(np.rint(py[t])) - half - search, int(np.rint(px[t])) - half - search
+                if top < 0 or left < 0 or top + L > h or left + L > w:
+                    continue
+                oy, ox, pk = ncc_peak(refimg[cy[t] - half:cy[t] + half, cx[t] - half:cx[t] + half],
+                                      img[top:top + L, left:left + L])
+                if pk >= min_peak:
+                    dx[t] = (left + search + half + ox) - w / 2 - X[t]
+                    dy[t] = (top + search + half + oy) - h / 2 - Y[t]
+            fit, nfit = fit_camera(dx, dy, X, Y)
+            if np.all(np.isfinite(fit)):
+                params[k], used[k], prev = fit, nfit, fit
+            else:
+                params[k], used[k] = prev, 0
+    return params, used, len(cx)

@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(HERE, 'libslipcam_b200.so')
 OK, EINVAL, ERUNTIME, ETIMEOUT = 0, 1, 2, 3
 GROSS_NONE, GROSS_FRAME, GROSS_WINDOW = 0, 1, 2
 FORM_AUTO, FORM_FFT32, FORM_TC = 0, 1, 2
+COARSE_MAX_WINDOWS = 2048
 
 
 class Params(ctypes.Structure):
@@ -46,6 +47,10 @@ SIGNATURES = {
                                ctypes.POINTER(_i)]),
     'b200_group_set_config': (_i, [_vp, _i, _i, _i, _i, _i]),
     'b200_periodicity_device': (_i, [_vp, _vp, _i, _vp, _vp]),
+    'b200_ncc_peaks_device': (_i, [_vp, _i, _i, _vp, _vp]),
+    'b200_coarse_track_device': (_i, [_vp, _vp, _i, _i, _vp, ctypes.c_double, _i, _vp, _vp, _vp, _vp, _vp]),
+    'b200_coarse_fit_device': (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _i, ctypes.c_double, _vp, _vp, _vp,
+                                    _vp]),
     'b200_frame_diff_device': (_i, [_vp, _i, _i, _i, _i, _vp, _vp, _vp]),
     'b200_chunk_std_median_device': (_i, [_vp, _i, _i, _i, _i, _i, _vp, _vp]),
     'b200_sobel_device': (_i, [_vp, _i, _i, _i, _vp, _vp]),

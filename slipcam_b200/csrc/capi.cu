@@ -27,6 +27,7 @@
 #include "multi.h"
 #include "periodicity.cuh"
 #include "scans.cuh"
+#include "stabilize.h"
 #include "sat.cuh"
 #include "tc_selftest.cuh"
 
@@ -130,6 +131,23 @@ void launch_corr(const CorrArgs &a, cudaStream_t s)
 {
     prepare<N>();
     corr_kernel<N, kThreads><<<unsigned(a.nwin) * a.nf, kThreads, Geo<N>::smem_bytes, s>>>(a);
+}
+
+// threads per pair of the latency-bound correlation (one frame of a chain at a time)
+constexpr int kLatencyThreads = 512;
+
+template <int N>
+void launch_corr_latency(const CorrArgs &a, cudaStream_t s)
+{
+    static bool done[64] = {};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        CK(cudaFuncSetAttribute(corr_latency_kernel<N, kLatencyThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(Geo<N>::smem_bytes)));
+        done[dev] = true;
+    }
+    corr_latency_kernel<N, kLatencyThreads><<<unsigned(a.nwin) * a.nf, kLatencyThreads, Geo<N>::smem_bytes, s>>>(a);
 }
 
 int g_num_sms[64] = {};
@@ -310,6 +328,9 @@ struct b200_handle {
     DevBuf<uint16_t> d_dtab;     // the FP16 DFT matrices of the tensor-core form
     DevBuf<int> d_status;        // device status word (3: a tensor-core wait gave up)
     DevBuf<CUtensorMap> d_tmaps; // TMA maps of the three denominator tables: slot 0, slot 1, device path
+    DevBuf<float> d_coarse;      // coarse tracking: one frame's surfaces and four outputs
+    DevBuf<double> d_cpeaks;     // coarse tracking: one frame's peaks
+    cudaEvent_t coarse_ev[5] = {};  // coarse tracking: tables ready (2), tables consumed (2), call start
     bool tc_ok = false;          // the geometry fits the tensor-core kernel
     int fpitch = 0;              // the pitch of the staged frames (a multiple of 16)
     bool profiling = false;      // events around the correlation launches
@@ -325,6 +346,8 @@ struct b200_handle {
             cudaEventDestroy(t.a);
             cudaEventDestroy(t.b);
         }
+        for (cudaEvent_t e : coarse_ev)
+            if (e) cudaEventDestroy(e);
         if (comp) cudaStreamDestroy(comp);
         if (copy) cudaStreamDestroy(copy);
     }
@@ -339,13 +362,37 @@ struct b200_handle {
                    uint32_t *sat, int64_t *sat2, float *dinv, float *offset, float *peak, float *snr,
                    float *cov, float *surface, cudaStream_t s)
     {
+        run_tables(frames, pitch, nf, sat, sat2, dinv, s);
+        run_corr(frames, pitch, nf, gross, gross_mode, sat, dinv, offset, peak, snr, cov, surface, form, s);
+        launches += 3;
+    }
+
+    // the summed-area tables and the variance denominators of nf frames
+    void run_tables(const uint8_t *frames, int pitch, int nf, uint32_t *sat, int64_t *sat2, float *dinv, cudaStream_t s)
+    {
         const int64_t fstride = int64_t(pitch) * height;
         launch_sat(frames, fstride, pitch, nf, height, width, sat, sat2, s);
         dinv_kernel<<<dim3(unsigned((width - W + 1 + 127) / 128), unsigned(height - W + 1), unsigned(nf)), 128, 0, s>>>(
             sat, sat2, sat_size(), height, width, W, dinv, dinv_size(), dpitch());
+    }
+
+    // the correlation of nf frames with their tables at sat / dinv, in the form `arith`
+    void run_corr(const uint8_t *frames, int pitch, int nf, const int32_t *gross, int gross_mode, const uint32_t *sat,
+                  const float *dinv, float *offset, float *peak, float *snr, float *cov, float *surface, int arith,
+                  cudaStream_t s)
+    {
+        const CorrArgs a = corr_args(frames, pitch, nf, gross, gross_mode, sat, dinv, offset, peak, snr, cov, surface);
+        run_corr_tail(a, nf, dinv, arith, s);
+    }
+
+    // the arguments of the correlation kernels for nf frames with their tables at sat / dinv
+    CorrArgs corr_args(const uint8_t *frames, int pitch, int nf, const int32_t *gross, int gross_mode,
+                       const uint32_t *sat, const float *dinv, float *offset, float *peak, float *snr, float *cov,
+                       float *surface) const
+    {
         CorrArgs a{};
         a.frames = frames;
-        a.fstride = fstride;
+        a.fstride = int64_t(pitch) * height;
         a.pitch = pitch;
         a.sat = sat;
         a.sat_fstride = sat_size();
@@ -375,6 +422,12 @@ struct b200_handle {
         a.snr = snr;
         a.cov = cov;
         a.surface = surface;
+        return a;
+    }
+
+    // the launch of run_corr (and its profiling events)
+    void run_corr_tail(const CorrArgs &a, int nf, const float *dinv, int arith, cudaStream_t s)
+    {
         Timed t{};
         if (profiling) {
             CK(cudaEventCreate(&t.a));
@@ -382,7 +435,7 @@ struct b200_handle {
             t.pairs = uint64_t(nf) * nwin;
             CK(cudaEventRecord(t.a, s));
         }
-        if (form == B200_FORM_TC) {
+        if (arith == B200_FORM_TC) {
             const uint4 *dt = reinterpret_cast<const uint4 *>(d_dtab.p);
             const int mi = dinv == slot[0].dinv.p ? 0 : dinv == slot[1].dinv.p ? 1 : 2;
             if (mi == 2 && dinv != d_dinv.p) fail(B200_EINVAL, "no TMA map for this denominator table");
@@ -398,7 +451,7 @@ struct b200_handle {
             CK(cudaEventRecord(t.b, s));
             timed.push_back(t);
         }
-        launches += 4;
+        launches += 1;
     }
 };
 
@@ -1013,6 +1066,84 @@ int b200_text_mask_device(const float *edge, const float *sd, int height, int wi
     fill_kernel<<<nb, 256, 0, s>>>(b, mask, n);
     if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return B200_ERUNTIME;
     return B200_OK;
+}
+
+int b200_coarse_track_device(b200_handle *h, const uint8_t *frames, int n, int pitch, const uint8_t *keep,
+                             double min_peak, int reset, int32_t *gross, double *prev, double *params, int32_t *used,
+                             void *stream)
+{
+    return guarded(h, [&] {
+        if (!h->ready) fail(B200_ERUNTIME, "set_reference first");
+        if (n < 0) fail(B200_EINVAL, "the number of frames must not be negative");
+        if (h->W % 2) fail(B200_EINVAL, "coarse tracking needs an even window");
+        if (h->nwin > B200_COARSE_MAX_WINDOWS)
+            fail(B200_EINVAL, "coarse tracking handles up to " + std::to_string(B200_COARSE_MAX_WINDOWS) + " windows");
+        if (!keep || !gross || !prev || (n && (!frames || !params || !used || pitch < h->width)))
+            fail(B200_EINVAL, "null input or output, or a pitch below the width");
+        CK(cudaSetDevice(h->device));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const size_t nwin = size_t(h->nwin), MM = size_t(h->M) * h->M;
+        if (reset) {
+            CK(cudaMemsetAsync(gross, 0, 2 * nwin * sizeof(int32_t), s));
+            CK(cudaMemsetAsync(prev, 0, 4 * sizeof(double), s));
+        }
+        if (n == 0) return;
+        // the big transform has no fused peak: its surfaces go through the peak kernel
+        const bool fused = h->N != kBigN;
+        const size_t work = nwin * (7 + (fused ? 0 : MM));
+        if (h->d_coarse.n < work) h->d_coarse.alloc(work);
+        if (h->d_cpeaks.n < 3 * nwin) h->d_cpeaks.alloc(3 * nwin);
+        if (!h->coarse_ev[0])
+            for (cudaEvent_t &e : h->coarse_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        float *o = h->d_coarse.p, *surf = fused ? nullptr : o + 7 * nwin;
+        const int64_t fstride = int64_t(pitch) * h->height;
+        FitArgs fa{h->d_cpeaks.p, gross, keep, h->d_down.p, h->d_across.p, h->W / 2, h->ny, h->nx, h->height,
+                   h->width, h->W, h->R, min_peak, prev, nullptr, nullptr};
+        // two sets of tables: those of group g + 1 are built on the side stream while the frames of
+        // group g are tracked on `stream` (the chain of one frame leaves most SMs idle)
+        uint32_t *sat[2] = {h->d_sat.p, h->slot[0].sat.p};
+        int64_t *sat2[2] = {h->d_sat2.p, h->slot[0].sat2.p};
+        float *dinv[2] = {h->d_dinv.p, h->slot[0].dinv.p};
+        cudaEvent_t *ready = h->coarse_ev, *consumed = h->coarse_ev + 2, start = h->coarse_ev[4];
+        cudaStream_t side = h->copy;
+        const int G = h->group, groups = (n + G - 1) / G;
+        auto tables = [&](int g) {
+            const int nf = std::min(G, n - g * G);
+            if (g >= 2) CK(cudaStreamWaitEvent(side, consumed[g % 2], 0));
+            h->run_tables(frames + int64_t(g) * G * fstride, pitch, nf, sat[g % 2], sat2[g % 2], dinv[g % 2], side);
+            CK(cudaGetLastError());
+            CK(cudaEventRecord(ready[g % 2], side));
+            h->launches += 3;
+        };
+        CK(cudaEventRecord(start, s));   // the frames and the state are written on `stream` before this call
+        CK(cudaStreamWaitEvent(side, start, 0));
+        tables(0);
+        for (int g = 0; g < groups; ++g) {
+            if (g + 1 < groups) tables(g + 1);
+            CK(cudaStreamWaitEvent(s, ready[g % 2], 0));
+            const int nf = std::min(G, n - g * G);
+            for (int j = 0; j < nf; ++j) {
+                const int f = g * G + j;
+                CorrArgs a = h->corr_args(frames + int64_t(f) * fstride, pitch, 1, gross, B200_GROSS_WINDOW,
+                                          sat[g % 2] + j * h->sat_size(), dinv[g % 2] + j * h->dinv_size(), o,
+                                          o + 2 * nwin, o + 3 * nwin, o + 4 * nwin, surf);
+                if (fused) {
+                    a.ncc = h->d_cpeaks.p;
+                    B200_DISPATCH(h->N, launch_corr_latency, a, s);
+                    CK(cudaGetLastError());
+                } else {
+                    h->run_corr_tail(a, 1, a.dinv, B200_FORM_FFT32, s);
+                    CK(launch_ncc_peaks(surf, int(nwin), h->M, h->d_cpeaks.p, s));
+                    h->launches += 1;
+                }
+                fa.params = params + 4 * size_t(f);
+                fa.used = used + f;
+                CK(launch_coarse_fit(fa, s));
+                h->launches += 2;
+            }
+            CK(cudaEventRecord(consumed[g % 2], s));
+        }
+    });
 }
 
 int b200_periodicity_device(b200_handle *h, const float *surface, int exclude, float *out, void *stream)

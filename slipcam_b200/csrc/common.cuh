@@ -63,6 +63,8 @@ struct CorrArgs {
     int gross_mode;            // 0 none, 1 per frame, 2 per window
     float *offset, *peak, *snr, *cov;   // nf x nwin (x 2, x 3), the pairs of this group
     float *surface;            // nullptr, or nf x nwin x M x M: the normalized surfaces
+    double *ncc;               // nullptr, or nf x nwin x 3: stabilize.ncc_peak's (dy, dx, value) of each
+                               // surface ((NaN, NaN, -inf) for an invalid pair)
 };
 
 }   // namespace b200

@@ -8,6 +8,7 @@
 #include <climits>
 
 #include "fft_passes.cuh"
+#include "ncc_peak.cuh"
 
 namespace b200 {
 
@@ -257,6 +258,10 @@ __device__ __forceinline__ void corr_pair(const CorrArgs &a, int k, int f, float
     // the reference's validity (cxx/cpu.cpp:121-125 with cxx/surface.h:39-45)
     if (!(norm > 0) || sy < 0 || sx < 0 || sy + L > a.h || sx + L > a.w) {
         if (threadIdx.x == 0) invalid_outputs(q, a.offset, a.peak, a.snr, a.cov);
+        if (a.ncc && threadIdx.x == 0) {
+            a.ncc[3 * q] = a.ncc[3 * q + 1] = NAN;
+            a.ncc[3 * q + 2] = -INFINITY;
+        }
         if (a.surface)
             for (int i = threadIdx.x; i < M * M; i += NT) a.surface[q * M * M + i] = 0.0f;
         return;
@@ -317,6 +322,7 @@ __device__ __forceinline__ void corr_pair(const CorrArgs &a, int k, int f, float
     __syncthreads();
     if (a.surface)
         for (int i = threadIdx.x; i < M * M; i += NT) a.surface[q * M * M + i] = Sr[size_t(i / M) * G::RP + i % M];
+    if (a.ncc) ncc_peak_block<NT>(Sr, G::RP, M, a.ncc + 3 * q);
 
     surface_peak<NT>(Sr, G::RP, M, R, a.stat, gy, gx, a.W * a.W, q, a.offset, a.peak, a.snr, a.cov, nullptr);
 }
@@ -325,6 +331,16 @@ __device__ __forceinline__ void corr_pair(const CorrArgs &a, int k, int f, float
 // CTAs of one window (one reference spectrum) run together and share it through L2
 template <int N, int NT>
 __global__ void __launch_bounds__(NT, (N <= 160 ? 2 : 1)) corr_kernel(CorrArgs a)
+{
+    extern __shared__ float4 smem_raw[];
+    corr_pair<N, NT>(a, blockIdx.x / a.nf, blockIdx.x % a.nf, reinterpret_cast<float2 *>(smem_raw));
+}
+
+// one frame's pairs when their latency is what counts (a frame chain where each frame waits for the
+// one before, a grid of a few dozen windows leaving most SMs idle): corr_kernel's work with NT
+// threads per pair and one CTA per SM allowed the registers of the larger block
+template <int N, int NT>
+__global__ void __launch_bounds__(NT, 1) corr_latency_kernel(CorrArgs a)
 {
     extern __shared__ float4 smem_raw[];
     corr_pair<N, NT>(a, blockIdx.x / a.nf, blockIdx.x % a.nf, reinterpret_cast<float2 *>(smem_raw));

@@ -1,0 +1,212 @@
+"""
+Coarse similarity tracking of the frames of a video on a reference frame, on the b200 backend:
+stabilize.coarse_track (python/slipcam/stabilize.py:54-96) with its ncc_peak (:22-44) and the robust
+fit slip_series.fit_camera (python/slipcam/slip_series.py:49-72); same arguments, same results.
+
+A grid of large windows of the reference frame (away from the burned-in text, not flat) is tracked in
+each frame around the positions predicted by the previous frame's transform. Per frame, three
+stream-ordered steps on the GPU and no host round trip:
+
+* the correlation of the grid's templates (FP32 FFT correlation, normalized surfaces), each
+  window's search window placed by the gross offsets on the device;
+* the peak of each surface, refined by a parabola per axis;
+* the robust similarity fit of the frame in float64, in one CTA, which writes the frame's transform
+  and the next frame's gross offsets.
+
+The frame loop runs in the library (b200_coarse_track_device): per group of frames the tables in one
+batch, then three launches per frame.
+
+Frames in host memory are staged through two page-locked buffers and copied on a side stream while
+the previous chunk is tracked; CUDA tensors are read in place.
+"""
+
+import ctypes
+
+import numpy as np
+
+from . import _lib, framecor
+
+
+def apply(params, x, y):
+    """The positions of the points (x, y), relative to the image center, under the similarity
+    transform params = (p, q, a, s): x' = x + p - a y + s x, y' = y + q + a x + s y
+    (stabilize.py:47-51)"""
+    p, q, a, s = params
+    return x + p - a * y + s * x, y + q + a * x + s * y
+
+
+def _check(rc):
+    if rc != _lib.OK:
+        raise (ValueError if rc == _lib.EINVAL else RuntimeError)(f'framecor: stabilize step failed ({rc})')
+
+
+def ncc_peaks(surfaces):
+    """The peak of each normalized surface (a float32 CUDA tensor ... x M x M) as ncc_peak gives it:
+    (dy, dx) relative to the surface centre, refined by a parabola per axis, and the value; a float64
+    CUDA tensor ... x 3."""
+    import torch
+    s = surfaces.to(torch.float32).contiguous()
+    M = s.shape[-1]
+    if s.dim() < 2 or s.shape[-2] != M:
+        raise ValueError('framecor: the surfaces must be ... x M x M')
+    n = s.numel() // (M * M) if M else 0
+    out = torch.empty(tuple(s.shape[:-2]) + (3,), dtype=torch.float64, device=s.device)
+    _check(_lib.lib().b200_ncc_peaks_device(s.data_ptr(), n, M, out.data_ptr(),
+                                            torch.cuda.current_stream(s.device).cuda_stream))
+    return out
+
+
+def template_grid(h, w, window, step, search):
+    """The centres of the rows and columns of windows of coarse_track (stabilize.py:61-63)"""
+    half = window // 2
+    return np.arange(search + half, h - search - half, step), np.arange(search + half, w - search - half, step)
+
+
+def _keep(ref, text, yc, xc, half):
+    """The windows without text and not flat (the standard deviation of the reference window above
+    2), ny x nx (stabilize.py:65-67)"""
+    refimg = np.asarray(ref).astype(np.float64)
+    text = np.asarray(text, bool)
+    keep = np.zeros((len(yc), len(xc)), bool)
+    for i, y in enumerate(yc):
+        for j, x in enumerate(xc):
+            keep[i, j] = (not text[y - half:y + half, x - half:x + half].any()
+                          and refimg[y - half:y + half, x - half:x + half].std() > 2)
+    return keep
+
+
+def _runs(order, chunk):
+    """order in pieces of at most chunk frames"""
+    return [order[k:k + chunk] for k in range(0, len(order), chunk)]
+
+
+class CoarseTracker:
+    """
+    The templates of coarse_track, prepared once: the grid of window x window templates of the
+    reference frame ref_frame (height x width uint8) centred search + window // 2 pixels or more inside
+    it, step apart, those without text (text: height x width bool) and not flat in use, their spectra
+    resident on the GPU. run() tracks a video's frames with them (stabilize.py:54-96).
+    """
+
+    def __init__(self, ref_frame, text, window=96, step=96, search=32, min_peak=0.5, device=None):
+        import torch
+        if window % 2 or window < 2:
+            raise ValueError('framecor: coarse_track needs an even window of at least 2 pixels')
+        ref_frame = ref_frame.cpu().numpy() if isinstance(ref_frame, torch.Tensor) else np.asarray(ref_frame)
+        text = text.cpu().numpy() if isinstance(text, torch.Tensor) else text
+        self.height, self.width = h, w = ref_frame.shape
+        self.window, self.search, self.min_peak = window, search, float(min_peak)
+        half = window // 2
+        self.yc, self.xc = template_grid(h, w, window, step, search)
+        keep = _keep(ref_frame, text, self.yc, self.xc, half)
+        self.count = int(keep.sum())
+        self.nwin = keep.size
+        self.device = torch.device('cuda', torch.cuda.current_device()) if device is None else torch.device(device)
+        self._cor = None
+        if self.nwin == 0:   # no window fits the frame
+            return
+        if self.nwin > _lib.COARSE_MAX_WINDOWS:
+            raise ValueError(f'framecor: coarse_track handles up to {_lib.COARSE_MAX_WINDOWS} windows, not {self.nwin}')
+        dev = self.device
+        self._cor = framecor.Correlator(h, w, self.yc - half, self.xc - half, window=window, search=search,
+                                        backend='b200', device=dev.index or 0)
+        with torch.cuda.device(dev):
+            self._cor.set_reference(torch.as_tensor(np.ascontiguousarray(ref_frame, np.uint8)).to(dev))
+            self._keep = torch.as_tensor(keep.astype(np.uint8).ravel()).to(dev)
+            self._gross = torch.zeros((self.nwin, 2), dtype=torch.int32, device=dev)
+            self._prev = torch.zeros(4, dtype=torch.float64, device=dev)
+
+    def run(self, frames, ref, start=0, chunk=64):
+        """(params, used, count) of coarse_track for the frames (n x height x width uint8, a numpy array
+        or a CUDA tensor) around the reference frame ref: forward from ref, then backward to start.
+        chunk: frames per call of the library (and per host-to-device copy)."""
+        import torch
+        n, h, w = frames.shape
+        if (h, w) != (self.height, self.width):
+            raise ValueError('framecor: the frames and the reference frame differ in size')
+        if not 0 <= ref < n:
+            raise IndexError('framecor: the reference frame is not in the video')
+        params = np.full((n, 4), np.nan)
+        used = np.zeros(n, int)
+        passes = [list(range(ref + 1, n)), list(range(ref - 1, start - 1, -1))]
+        order = passes[0] + passes[1]
+        params[ref], used[ref] = 0, self.count
+        if self._cor is None:   # no window: no fit anywhere, the transforms stay zero
+            params[order] = 0
+            return params, used, self.count
+        dev = self.device
+        with torch.cuda.device(dev):
+            out = torch.full((len(order), 4), float('nan'), dtype=torch.float64, device=dev)   # in tracking order
+            nused = torch.zeros(len(order), dtype=torch.int32, device=dev)
+            stream = torch.cuda.current_stream(dev)
+
+            def track(ptr, m, at, reset):
+                """m frames at ptr (in tracking order), outputs from row `at` of the order"""
+                _lib.raise_for(_lib.lib().b200_coarse_track_device(
+                    self._cor._h, ptr, m, w, self._keep.data_ptr(), ctypes.c_double(self.min_peak), int(reset),
+                    self._gross.data_ptr(), self._prev.data_ptr(), out[at:].data_ptr(), nused[at:].data_ptr(),
+                    stream.cuda_stream), self._cor._h)
+
+            at = 0
+            if isinstance(frames, torch.Tensor) and frames.is_cuda:
+                f = frames.to(torch.uint8).contiguous()
+                for frames_in_order in passes:
+                    for c, run in enumerate(_runs(frames_in_order, chunk)):
+                        if run[0] < run[-1] or len(run) == 1:   # forward: the frames as they lie
+                            track(f[run[0]].data_ptr(), len(run), at, c == 0)
+                        else:                                    # backward: a reversed copy of the chunk
+                            rev = f[run[-1]:run[0] + 1].flip(0).contiguous()
+                            track(rev.data_ptr(), len(run), at, c == 0)
+                        at += len(run)
+            elif order:
+                C = min(chunk, len(order))
+                host = [torch.empty((C, h, w), dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+                devb = [torch.empty((C, h, w), dtype=torch.uint8, device=dev) for _ in range(2)]
+                copy = torch.cuda.Stream(dev)
+                done = [None, None]
+                b = 0
+                for frames_in_order in passes:
+                    for c, run in enumerate(_runs(frames_in_order, C)):
+                        if done[b] is not None:
+                            done[b].synchronize()   # the chunk before last is tracked: both buffers b are free
+                        dst = host[b].numpy()[:len(run)]
+                        if run[0] <= run[-1]:
+                            np.copyto(dst, frames[run[0]:run[-1] + 1])
+                        elif run[-1] > 0:
+                            np.copyto(dst, frames[run[0]:run[-1] - 1:-1])
+                        else:
+                            np.copyto(dst, frames[run])
+                        with torch.cuda.stream(copy):
+                            devb[b][:len(run)].copy_(host[b][:len(run)], non_blocking=True)
+                            ready = copy.record_event()
+                        stream.wait_event(ready)
+                        track(devb[b].data_ptr(), len(run), at, c == 0)
+                        done[b] = stream.record_event()
+                        at += len(run)
+                        b ^= 1
+            if order:
+                params[order] = out.cpu().numpy()
+                used[order] = nused.cpu().numpy()
+        return params, used, self.count
+
+
+def coarse_track(frames, ref, text, window=96, step=96, search=32, min_peak=0.5, start=0, *, chunk=64):
+    """The similarity transform of each frame relative to the frame ref (frames x 4: p, q, a, s about
+    the image center), the number of windows of each frame's fit, and the number of windows of the
+    grid in use (stabilize.py:54-96). frames: n x height x width uint8, a numpy array (memory-mapped
+    or not) or a CUDA tensor; text: the burned-in text mask (height x width bool). The frames after
+    ref are tracked forward from it, then those from ref - 1 down to start backward; each frame is
+    predicted from the previous one's transform (zero at the start of each pass). A frame without a
+    fit (fewer than 4 windows) keeps the previous transform and counts 0 windows; the frames before
+    start stay NaN.
+
+    chunk: frames per call of the library (and per host-to-device copy). The correlation is the FP32
+    form. The window must be even (the reference's template is 2 (window // 2) pixels wide)."""
+    import torch
+    if window % 2 or window < 2:
+        raise ValueError('framecor: coarse_track needs an even window of at least 2 pixels')
+    if not 0 <= ref < len(frames):
+        raise IndexError('framecor: the reference frame is not in the video')
+    dev = frames.device if isinstance(frames, torch.Tensor) and frames.is_cuda else None
+    tracker = CoarseTracker(frames[ref], text, window=window, step=step, search=search, min_peak=min_peak, device=dev)
+    return tracker.run(frames, ref, start=start, chunk=chunk)

@@ -18,6 +18,12 @@ Workloads (sizes as named):
              stripes; grids 32/16, 64/48, 128/64 (skip 16); per-window gross U[-20, 20]
   stream     1000 x 1080 x 1920, sigma 2, noise 3 DN, a 5 Hz 4 px shake plus a random walk, a
              60 px fault step over 30 frames; window 64, search 64, skip 8
+  camera     a camera moving over a textured scene (default 24 x 240 x 320; 720 x 1280 for the
+             stabilize workload): frame k shows the scene through the similarity transform
+             params[k] = (p, q, a, s) about the image centre (the content at x of the reference
+             frame appears at x + p - a y + s x, y + q + a x + s y), a random walk from the
+             reference frame, bicubic resampling, burned-in text boxes fixed in the frame, optional
+             blank frames; for stabilize.coarse_track
   shifts_f32 float32 frames (default 41 x 256 x 256), sigma 2, frame k moved as a whole by a
              continuous shift U[-3, 3] px per axis (frame 0 unmoved: the reference), optional
              Gaussian noise, not rounded; window 64, search 8, skip 32 (the differentiable path)
@@ -181,3 +187,67 @@ def shifts_f32(n=41, h=256, w=256, seed=4, noise=0.0, max_shift=3.0):
             img = img + rng.standard_normal(img.shape) * noise
         frames[k] = img
     return frames, shifts
+
+
+def camera(n=24, h=240, w=320, *, ref=0, seed=6, sigma=2.0, noise=1.0, walk=(2.0, 2.0, 0.003, 0.003),
+           text=((40, 8, 200, 24),), flat=None, blank=(), device=None):
+    """A camera moving over a textured scene. Returns frames (n, h, w) uint8 (a CUDA tensor when
+    device is given), params (n, 4) float64 (params[ref] = 0, a random walk of steps N(0, walk)
+    away from it both ways) and the text mask (h, w) bool. text: boxes (x0, y0, x1, y1) drawn in
+    every frame at the same place (a bright outline around dark strokes); flat: a box (x0, y0, x1,
+    y1) of the scene made uniform (100 DN); blank: frames replaced by a uniform 128 DN."""
+    rng = np.random.default_rng(seed)
+    pad = 64 + int(4 * max(walk[0], walk[1]) * math.sqrt(n))
+    tex = texture(h + 2 * pad, w + 2 * pad, sigma, rng)
+    if flat is not None:
+        x0, y0, x1, y1 = flat
+        tex[y0 + pad:y1 + pad, x0 + pad:x1 + pad] = 100.0
+    steps = rng.normal(0.0, 1.0, (n, 4)) * np.asarray(walk, np.float64)
+    params = np.zeros((n, 4))
+    for k in range(ref + 1, n):
+        params[k] = params[k - 1] + steps[k]
+    for k in range(ref - 1, -1, -1):
+        params[k] = params[k + 1] + steps[k]
+    mask = np.zeros((h, w), bool)
+    for x0, y0, x1, y1 in text:
+        mask[y0:y1, x0:x1] = True
+    if device is None:
+        from scipy import ndimage
+        coef = ndimage.spline_filter(tex, order=3)
+        yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+        yy -= h / 2
+        xx -= w / 2
+    else:
+        import torch
+        t = torch.as_tensor(tex, dtype=torch.float32, device=device)[None, None]
+        yy, xx = torch.meshgrid(torch.arange(h, device=device, dtype=torch.float64) - h / 2,
+                                torch.arange(w, device=device, dtype=torch.float64) - w / 2, indexing='ij')
+    frames = np.empty((n, h, w), np.uint8)
+    for k in range(n):
+        p, q, a, s = params[k]
+        # the scene point seen at frame pixel z: the inverse of z = (1 + s, -a; a, 1 + s) x + (p, q)
+        det = (1 + s) ** 2 + a ** 2
+        zx, zy = xx - p, yy - q
+        sx = ((1 + s) * zx + a * zy) / det + w / 2 + pad
+        sy = (-a * zx + (1 + s) * zy) / det + h / 2 + pad
+        if device is None:
+            img = ndimage.map_coordinates(coef, [sy, sx], order=3, mode='nearest', prefilter=False)
+        else:
+            import torch
+            g = torch.stack([sx / (w + 2 * pad - 1) * 2 - 1, sy / (h + 2 * pad - 1) * 2 - 1], -1)
+            img = torch.nn.functional.grid_sample(t, g[None].float(), mode='bicubic', padding_mode='border',
+                                                  align_corners=True)[0, 0].double().cpu().numpy()
+        if noise:
+            img = img + rng.standard_normal((h, w)) * noise
+        for x0, y0, x1, y1 in text:
+            img[y0:y1, x0:x1] = 30.0
+            img[y0:y0 + 2, x0:x1] = img[y1 - 2:y1, x0:x1] = 240.0
+            img[y0:y1, x0:x0 + 2] = img[y0:y1, x1 - 2:x1] = 240.0
+            img[y0 + 4:y1 - 4:4, x0 + 4:x1 - 4] = 220.0
+        if k in blank:
+            img = np.full((h, w), 128.0)
+        frames[k] = np.clip(np.rint(img), 0, 255).astype(np.uint8)
+    if device is not None:
+        import torch
+        return torch.as_tensor(frames).to(device), params, mask
+    return frames, params, mask
