@@ -19,7 +19,7 @@ namespace b200 {
 namespace {
 
 constexpr int kPeakThreads = 256;
-constexpr int kFitThreads = 512;
+constexpr int kFitThreads = 256;
 constexpr int kFitWarps = kFitThreads / 32;
 constexpr int kGrossLimit = 1 << 29;   // a predicted position beyond this is outside every frame
 
@@ -50,9 +50,10 @@ __device__ double median_by_rank(const double *v, int m, int n, double *sel)
         const double x = v[i];
         if (!(x < INFINITY)) continue;
         int rank = 0;
+#pragma unroll 8
         for (int j = 0; j < m; ++j) {
             const double y = v[j];
-            rank += (y < x) || (y == x && j < i);
+            rank += (y < x) | ((y == x) & (j < i));
         }
         if (rank == lo) sel[0] = x;
         if (rank == hi) sel[1] = x;
@@ -120,38 +121,33 @@ __global__ void __launch_bounds__(kFitThreads) coarse_fit_kernel(FitArgs a)
     for (int it = 0; it < 3 && !failed; ++it) {
         // the least squares of dx = p - a Y + s X, dy = q + a X + s Y over the windows in use, in
         // closed form: about the means, s and a are the projections of the centred offsets on the
-        // centred positions (x, y) and (-y, x); p and q restore the means
-        double s1[5] = {};
-        int cnt = 0;
+        // centred positions (x, y) and (-y, x); p and q restore the means. One reduction of the
+        // raw moments (the grid is near the image centre: centring them after the sums loses
+        // nothing that matters at these magnitudes)
+        double t[8] = {};
         for (int k = threadIdx.x; k < nwin; k += kFitThreads) {
             if (!use[k]) continue;
-            ++cnt;
-            s1[0] += a.xc[k % a.nx] + a.coff - hw;
-            s1[1] += a.yc[k / a.nx] + a.coff - hh;
-            s1[2] += d[k];
-            s1[3] += d[nwin + k];
+            const double X = a.xc[k % a.nx] + a.coff - hw, Y = a.yc[k / a.nx] + a.coff - hh, dx = d[k], dy = d[nwin + k];
+            t[0] += 1;
+            t[1] += X;
+            t[2] += Y;
+            t[3] += dx;
+            t[4] += dy;
+            t[5] += X * X + Y * Y;
+            t[6] += X * dx + Y * dy;
+            t[7] += X * dy - Y * dx;
         }
-        s1[4] = cnt;
-        block_sum<5>(s1, red, tot);
-        const int nuse_it = int(tot[4]);
+        block_sum<8>(t, red, tot);
+        const int nuse_it = int(tot[0]);
         if (2 * nuse_it < 8) {   // fewer than 8 rows in use
             failed = true;
             break;
         }
-        const double mx = tot[0] / nuse_it, my = tot[1] / nuse_it, mdx = tot[2] / nuse_it, mdy = tot[3] / nuse_it;
-        __syncthreads();
-        double s2[3] = {};
-        for (int k = threadIdx.x; k < nwin; k += kFitThreads) {
-            if (!use[k]) continue;
-            const double x = a.xc[k % a.nx] + a.coff - hw - mx, y = a.yc[k / a.nx] + a.coff - hh - my;
-            const double ex = d[k] - mdx, ey = d[nwin + k] - mdy;
-            s2[0] += x * x + y * y;
-            s2[1] += x * ex + y * ey;
-            s2[2] += x * ey - y * ex;
-        }
-        block_sum<3>(s2, red, tot);
         if (threadIdx.x == 0) {
-            const double sc = tot[1] / tot[0], rot = tot[2] / tot[0];
+            const double n = nuse_it, mx = tot[1] / n, my = tot[2] / n, mdx = tot[3] / n, mdy = tot[4] / n;
+            const double sxx = tot[5] - n * (mx * mx + my * my);
+            const double sc = (tot[6] - n * (mx * mdx + my * mdy)) / sxx;
+            const double rot = (tot[7] - n * (mx * mdy - my * mdx)) / sxx;
             m[0] = mdx + rot * my - sc * mx;
             m[1] = mdy - rot * mx - sc * my;
             m[2] = rot;
