@@ -563,6 +563,24 @@ def run_stabilize(args):
     po, uo, _ = oracle.coarse_track(host[:cpu_frames + 1], 0, text)
     cpu_s = time.perf_counter() - t
     err = np.abs(p - truth)
+    # the resampling half (stabilize.stabilize): the frames warped onto the reference with the
+    # tracked transforms, the text blanked
+    st = stabilize.Stabilizer(text)
+    for _ in range(args.warmup):
+        st.run(frames, p)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        warped, union = st.run(frames, p)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_w = e0.elapsed_time(e1) / steps
+    t = time.perf_counter()
+    stabilize.stabilize(host, p, text)
+    e2e_w = time.perf_counter() - t
+    t = time.perf_counter()
+    ow, _ = oracle.stabilize(host[:2], p[:2], text)
+    cpu_w = time.perf_counter() - t
     print(json.dumps({
         'metric': 'frames/s, coarse similarity tracking of a 720p video (stabilize.coarse_track defaults)',
         'value': (n - 1) / (ms / 1e3), 'unit': 'frames/s', 'n_gpus': 1, 'steps': steps, 'warmup': args.warmup,
@@ -579,6 +597,12 @@ def run_stabilize(args):
                       'used_equal': bool(np.array_equal(uo[1:], u[1:cpu_frames + 1])),
                       'host_equals_device': bool(np.array_equal(pe, p))},
         'error_vs_truth': {'shift_px': float(err[:, :2].max()), 'rotation_scale': float(err[:, 2:].max())},
+        'resample': {'what': 'stabilize.stabilize: text blanked (31 px box means), frames warped (bilinear), text union',
+                     'value': n / (ms_w / 1e3), 'unit': 'frames/s', 'ms_per_step': ms_w,
+                     'e2e': {'value': n / e2e_w, 'unit': 'frames/s', 'path': 'stabilize.stabilize over a host array'},
+                     'cpu_baseline': {'value': 2 / cpu_w, 'unit': 'frames/s', 'cores': 1, 'kind': 'port',
+                                      'sample': f'2 frames ({cpu_w:.2f} s)'},
+                     'equals_oracle': bool(np.array_equal(warped[:2].cpu().numpy(), ow))},
     }))
 
 

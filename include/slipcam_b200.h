@@ -211,6 +211,34 @@ B200_API int b200_coarse_track_device(b200_handle *h, const uint8_t *frames, int
                                       double min_peak, int reset, int32_t *gross, double *prev, double *params,
                                       int32_t *used, void *stream);
 
+/* ---- The resampling of stabilize (python/slipcam/stabilize.py:99-124): frames warped onto the
+ * reference under their similarity transforms, the burned-in text blanked first, the text mask
+ * warped too. The arithmetic is the reference's: scipy.ndimage.uniform_filter's box means (axis 0
+ * then axis 1, float32 between the passes, borders reflected), numpy's float32 mean (its pairwise
+ * summation tree), map_coordinates' bilinear interpolation (order 1, mode 'constant', a coordinate
+ * outside [0, n - 1] taking the fill).
+ *
+ * b200_stab_create: a context for frames of height x width with the text mask `text` (host memory,
+ * height x width bytes, nonzero = text) and the blanking box of size x size pixels (31 in the
+ * reference): the mask, its box mean and the summation plans on `device`. */
+typedef struct b200_stab b200_stab;
+B200_API int b200_stab_create(int height, int width, const uint8_t *text, int size, int device, b200_stab **out);
+B200_API int b200_stab_destroy(b200_stab *s);
+B200_API const char *b200_stab_last_error(const b200_stab *s);
+
+/* stabilize's frame loop (stabilize.py:117-123) on n device frames (uint8, rows `pitch` bytes apart,
+ * frames pitch * height apart) with their transforms params (device, n x 4 doubles p, q, a, s):
+ * out (device, n x height x width bytes) = uint8(clip(warp(blanked frame, params[k]), 0, 255)),
+ * the fill the blanked frame's mean; union_mask (device, height x width bytes; may be NULL) gets 1
+ * where a frame's warped text mask exceeds 0.5 (the caller zeroes it first). Stream-ordered. */
+B200_API int b200_stab_frames_device(b200_stab *s, const uint8_t *frames, int n, int pitch, const double *params,
+                                     uint8_t *out, uint8_t *union_mask, void *stream);
+
+/* stabilize.warp (stabilize.py:99-106) of one float32 frame (device, height x width) with the
+ * transform params (device, 4 doubles) and the fill value: out (device, float32). */
+B200_API int b200_warp_f32_device(const float *frame, int height, int width, const double *params, float fill,
+                                  float *out, void *stream);
+
 /* ---- The frame scans of auto_slip (python/slipcam/auto_slip.py:56-94), on device memory. Frames
  * are uint8, rows `pitch` bytes apart, frames pitch * height bytes apart.
  * b200_frame_diff_device: out[k] = the mean |frames[k + 1] - frames[k]| over the pixels, k < n - 1

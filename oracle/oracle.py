@@ -376,3 +376,87 @@ def coarse_track(frames, ref, text, window=96, step=96, search=32, min_peak=0.5,
             else:
                 params[k], used[k] = prev, 0
     return params, used, len(cx)
+
+
+def _box_mean_1d(x, size, axis):
+    """the box mean over `size` along `axis`, borders reflected (half-sample), float32 results from
+    the window sums in float64 (exact for these values) divided by size"""
+    x = np.moveaxis(np.asarray(x, np.float32), axis, -1).astype(np.float64)
+    n = x.shape[-1]
+    s1 = size // 2
+    idx = np.arange(-s1, n + size - s1 - 1)
+    idx = np.mod(idx, 2 * n)
+    idx = np.where(idx < n, idx, 2 * n - 1 - idx)
+    ext = x[..., idx]
+    c = np.concatenate([np.zeros(x.shape[:-1] + (1,)), np.cumsum(ext, -1)], -1)
+    out = ((c[..., size:size + n] - c[..., :n]) / size).astype(np.float32)
+    return np.moveaxis(out, -1, axis)
+
+
+def box_mean(x, size=31):
+    """
+    TEST INFRASTRUCTURE. The restatement of scipy.ndimage.uniform_filter(x, size) on a float32 image
+    as stabilize.py:116-120 uses it: along axis 0, rounded to float32, then along axis 1.
+    """
+    return _box_mean_1d(_box_mean_1d(x, size, 0), size, 1)
+
+
+def bilinear(img, cy, cx, cval):
+    """map_coordinates(img, [cy, cx], order=1, mode='constant', cval): float64 weights, a coordinate
+    outside [0, n - 1] (or NaN) taking cval, the result rounded to float32"""
+    img = np.asarray(img, np.float32).astype(np.float64)
+    h, w = img.shape
+    cy, cx = np.asarray(cy, np.float64), np.asarray(cx, np.float64)
+    inside = (cy >= 0) & (cy <= h - 1) & (cx >= 0) & (cx <= w - 1)
+    y = np.where(inside, cy, 0.0)
+    x = np.where(inside, cx, 0.0)
+    y0, x0 = np.floor(y), np.floor(x)
+    ty, tx = y - y0, x - x0
+    y0, x0 = y0.astype(np.int64), x0.astype(np.int64)
+    y1, x1 = np.minimum(y0 + 1, h - 1), np.minimum(x0 + 1, w - 1)
+    v = (img[y0, x0] * (1 - ty) * (1 - tx) + img[y0, x1] * (1 - ty) * tx
+         + img[y1, x0] * ty * (1 - tx) + img[y1, x1] * ty * tx)
+    return np.where(inside, v, np.float64(np.float32(cval))).astype(np.float32)
+
+
+def warp(frame, params, fill=None):
+    """
+    TEST INFRASTRUCTURE. The restatement of stabilize.warp (python/slipcam/stabilize.py:99-106): each
+    pixel (x, y) of the reference takes the frame's value at the similarity transform of (x, y)
+    about the image centre, bilinear, outside the frame the fill (default numpy's mean of the frame).
+    """
+    f = np.asarray(frame)
+    h, w = f.shape
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    x, y = xx - w / 2, yy - h / 2
+    p, q, a, s = np.asarray(params, np.float64)
+    sx = x + p - a * y + s * x
+    sy = y + q + a * x + s * y
+    fill = f.mean() if fill is None else fill
+    return bilinear(f.astype(np.float32), sy + h / 2, sx + w / 2, fill)
+
+
+def stabilize(frames, params, text, size=31):
+    """
+    TEST INFRASTRUCTURE. The restatement of stabilize.stabilize (python/slipcam/stabilize.py:109-124):
+    per frame, the text pixels replaced by the box mean of the pixels without text around them
+    (divided by the box mean of the mask, floored at 1e-3; the mean of the frame's pixels without
+    text where that mean is 1e-3 or less), warped onto the reference, clipped and cast to uint8;
+    and the union of the warped text masks above 0.5.
+    """
+    f_all = np.asarray(frames)
+    n, h, w = f_all.shape
+    text = np.asarray(text, bool)
+    keep = (~text).astype(np.float32)
+    den = box_mean(keep, size)
+    out = np.empty((n, h, w), np.uint8)
+    union = np.zeros((h, w), bool)
+    floor = np.float32(1e-3)
+    for k in range(n):
+        f = f_all[k].astype(np.float32)
+        if text.any():
+            local = box_mean(f * keep, size) / np.maximum(den, floor)
+            f = np.where(text, np.where(den > floor, local, f[~text].mean()), f)
+        out[k] = np.clip(warp(f, params[k]), 0, 255).astype(np.uint8)
+        union |= warp(text.astype(np.float32), params[k], fill=0) > 0.5
+    return out, union

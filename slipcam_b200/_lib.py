@@ -48,6 +48,11 @@ SIGNATURES = {
     'b200_group_set_config': (_i, [_vp, _i, _i, _i, _i, _i]),
     'b200_periodicity_device': (_i, [_vp, _vp, _i, _vp, _vp]),
     'b200_ncc_peaks_device': (_i, [_vp, _i, _i, _vp, _vp]),
+    'b200_stab_create': (_i, [_i, _i, _vp, _i, _i, ctypes.POINTER(_vp)]),
+    'b200_stab_destroy': (_i, [_vp]),
+    'b200_stab_last_error': (ctypes.c_char_p, [_vp]),
+    'b200_stab_frames_device': (_i, [_vp, _vp, _i, _i, _vp, _vp, _vp, _vp]),
+    'b200_warp_f32_device': (_i, [_vp, _i, _i, _vp, ctypes.c_float, _vp, _vp]),
     'b200_coarse_track_device': (_i, [_vp, _vp, _i, _i, _vp, ctypes.c_double, _i, _vp, _vp, _vp, _vp, _vp]),
     'b200_coarse_fit_device': (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _i, ctypes.c_double, _vp, _vp, _vp,
                                     _vp]),

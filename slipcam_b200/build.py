@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, 'csrc')
 LIB = os.path.join(HERE, 'libslipcam_b200.so')
-SOURCES = ['capi.cu', 'diff.cu', 'multi.cu', 'stabilize.cu']
+SOURCES = ['capi.cu', 'diff.cu', 'multi.cu', 'stabilize.cu', 'warp.cu']
 NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 FLAGS = ['-std=c++17', '-O3', '--expt-relaxed-constexpr', '-gencode', 'arch=compute_100a,code=sm_100a',
          '-lineinfo', '-Xcompiler', '-fPIC', '-Xcompiler', '-fvisibility=hidden', '-diag-suppress', '20014']

@@ -18,6 +18,10 @@ batch, then three launches per frame.
 
 Frames in host memory are staged through two page-locked buffers and copied on a side stream while
 the previous chunk is tracked; CUDA tensors are read in place.
+
+The resampling half of the module, warp and stabilize (stabilize.py:99-124), runs on the GPU too
+(csrc/warp.cu): the text blanked with scipy's box means, the frames warped with map_coordinates'
+bilinear rule, the fill numpy's float32 mean, each step in the reference's arithmetic.
 """
 
 import ctypes
@@ -210,3 +214,114 @@ def coarse_track(frames, ref, text, window=96, step=96, search=32, min_peak=0.5,
     dev = frames.device if isinstance(frames, torch.Tensor) and frames.is_cuda else None
     tracker = CoarseTracker(frames[ref], text, window=window, step=step, search=search, min_peak=min_peak, device=dev)
     return tracker.run(frames, ref, start=start, chunk=chunk)
+
+
+def _stab_check(rc, ctx):
+    if rc != _lib.OK:
+        msg = _lib.lib().b200_stab_last_error(ctx).decode() if ctx else ''
+        raise (ValueError if rc == _lib.EINVAL else RuntimeError)(msg or f'framecor: stabilize failed ({rc})')
+
+
+def warp(frame, params, fill=None):
+    """The frame resampled onto the reference (stabilize.py:99-106): the value at (x, y) of the
+    reference is that of the frame at the transformed position (bilinear); outside the frame, fill
+    (default: the frame's mean, numpy's). frame: height x width, a numpy array or a CUDA tensor;
+    returns float32 of the same kind."""
+    import torch
+    on_device = isinstance(frame, torch.Tensor) and frame.is_cuda
+    if fill is None:
+        fill = frame.double().mean().item() if on_device else np.asarray(frame).mean()
+    dev = frame.device if on_device else torch.device('cuda', torch.cuda.current_device())
+    f = (frame if on_device else torch.as_tensor(np.ascontiguousarray(frame, np.float32))).to(dev, torch.float32).contiguous()
+    if f.dim() != 2:
+        raise ValueError('framecor: the frame must be height x width')
+    h, w = f.shape
+    p = torch.as_tensor(np.asarray(params, np.float64).reshape(4)).to(dev)
+    out = torch.empty((h, w), dtype=torch.float32, device=dev)
+    with torch.cuda.device(dev):
+        _check(_lib.lib().b200_warp_f32_device(f.data_ptr(), h, w, p.data_ptr(), ctypes.c_float(float(np.float32(fill))),
+                                               out.data_ptr(), torch.cuda.current_stream(dev).cuda_stream))
+    return out if on_device else out.cpu().numpy()
+
+
+class Stabilizer:
+    """
+    stabilize's context for one text mask (height x width bool; numpy or torch): the mask, its box
+    mean over size x size pixels and the summation plans, on the GPU. run(frames, params) warps
+    frames onto the reference (stabilize.py:109-124).
+    """
+
+    def __init__(self, text, size=31, device=None):
+        import torch
+        text = text.cpu().numpy() if isinstance(text, torch.Tensor) else np.asarray(text)
+        if text.ndim != 2:
+            raise ValueError('framecor: the text mask must be height x width')
+        self.height, self.width = text.shape
+        self.device = torch.device('cuda', torch.cuda.current_device()) if device is None else torch.device(device)
+        t = np.ascontiguousarray(text.astype(bool), np.uint8)
+        ctx = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            rc = _lib.lib().b200_stab_create(self.height, self.width, t.ctypes.data, int(size), self.device.index or 0,
+                                             ctypes.byref(ctx))
+        _stab_check(rc, None)
+        self._ctx = ctx
+
+    def __del__(self):
+        ctx = getattr(self, '_ctx', None)
+        self._ctx = None
+        if ctx and _lib is not None and _lib._lib is not None:
+            _lib._lib.b200_stab_destroy(ctx)
+
+    def run(self, frames, params, chunk=64):
+        """(frames warped onto the reference, uint8, with their text blanked; the union of the warped
+        text masks, bool) for frames (n x height x width uint8, numpy or CUDA tensor) and params
+        (n x 4: p, q, a, s). Numpy in, numpy out; a CUDA tensor in, CUDA tensors out."""
+        import torch
+        n, h, w = frames.shape
+        if (h, w) != (self.height, self.width):
+            raise ValueError('framecor: the frames and the text mask differ in size')
+        params = params.cpu().numpy() if isinstance(params, torch.Tensor) else np.asarray(params)
+        if params.shape != (n, 4):
+            raise ValueError('framecor: params must be frames x 4')
+        dev = self.device
+        on_device = isinstance(frames, torch.Tensor) and frames.is_cuda
+        with torch.cuda.device(dev):
+            stream = torch.cuda.current_stream(dev)
+            p = torch.as_tensor(np.ascontiguousarray(params, np.float64)).to(dev)
+            union = torch.zeros((h, w), dtype=torch.uint8, device=dev)
+            lib = _lib.lib()
+
+            def run(src, m, k0, dst):
+                _stab_check(lib.b200_stab_frames_device(self._ctx, src.data_ptr(), m, w, p[k0:].data_ptr(),
+                                                        dst.data_ptr(), union.data_ptr(), stream.cuda_stream), self._ctx)
+
+            if on_device:
+                f = frames.to(dev, torch.uint8).contiguous()
+                out = torch.empty((n, h, w), dtype=torch.uint8, device=dev)
+                if n:
+                    run(f, n, 0, out)
+                return out, union.bool()
+            out = np.empty((n, h, w), np.uint8)
+            C = max(1, min(chunk, n))
+            host_in = torch.empty((C, h, w), dtype=torch.uint8, pin_memory=True)
+            host_out = torch.empty((C, h, w), dtype=torch.uint8, pin_memory=True)
+            dev_in = torch.empty((C, h, w), dtype=torch.uint8, device=dev)
+            dev_out = torch.empty((C, h, w), dtype=torch.uint8, device=dev)
+            for k0 in range(0, n, C):
+                m = min(C, n - k0)
+                np.copyto(host_in.numpy()[:m], frames[k0:k0 + m])
+                dev_in[:m].copy_(host_in[:m], non_blocking=True)
+                run(dev_in, m, k0, dev_out)
+                host_out[:m].copy_(dev_out[:m], non_blocking=True)
+                stream.synchronize()
+                out[k0:k0 + m] = host_out.numpy()[:m]
+            return out, union.cpu().numpy().astype(bool)
+
+
+def stabilize(frames, params, text, *, chunk=64):
+    """The frames warped onto the reference (uint8), with their text blanked (the local mean), and the
+    union of the warped text masks (stabilize.py:109-124). frames: n x height x width uint8 (numpy or
+    CUDA tensor); params: n x 4 (coarse_track's transforms); text: height x width bool."""
+    import torch
+    dev = frames.device if isinstance(frames, torch.Tensor) and frames.is_cuda else None
+    return Stabilizer(text, device=dev).run(frames, params, chunk=chunk)

@@ -1,6 +1,7 @@
 """
-Golden vectors of stabilize.coarse_track and stabilize.ncc_peak (python/slipcam/stabilize.py:22-96,
-with slip_series.fit_camera, python/slipcam/slip_series.py:49-72): the reference functions
+Golden vectors of stabilize.coarse_track, stabilize.ncc_peak, stabilize.warp and stabilize.stabilize
+(python/slipcam/stabilize.py:22-124, with slip_series.fit_camera, python/slipcam/slip_series.py:49-72):
+the reference functions
 themselves, taken from the reference's source by name (slip_series imports matplotlib, which is not
 installed) and run with numpy and scipy on seeded synthetic videos of a moving camera
 (slipcam_b200.synth.camera). Writes tests/golden/stabilize.npz. Run here, where the reference is
@@ -33,11 +34,12 @@ def reference_functions(root):
     py = os.path.join(root, 'python', 'slipcam')
     ns = {'np': np, 'ndimage': ndimage, 'signal': signal}
     _functions(os.path.join(py, 'slip_series.py'), ['fit_camera'], ns)
-    return _functions(os.path.join(py, 'stabilize.py'), ['ncc_peak', 'apply', 'coarse_track'], ns)[::2] + [ns['fit_camera']]
+    fns = _functions(os.path.join(py, 'stabilize.py'), ['ncc_peak', 'apply', 'coarse_track', 'warp', 'stabilize'], ns)
+    return fns[0], fns[2], ns['fit_camera'], fns[3], fns[4]
 
 
 def main(root):
-    ncc_peak, coarse_track, fit_camera = reference_functions(root)
+    ncc_peak, coarse_track, fit_camera, warp, stabilize = reference_functions(root)
     out = {}
     # a small grid: 48-px windows 40 px apart, +-12 px search; a flat patch, text, a blank frame
     f, p, m = synth.camera(12, 240, 320, ref=4, seed=6, flat=(236, 150, 300, 232), blank=(9,))
@@ -71,6 +73,19 @@ def main(root):
     dx[8:10] = np.nan
     fit, nfit = fit_camera(dx, dy, x, y)
     out.update(fit_dx=dx, fit_dy=dy, fit_x=x, fit_y=y, fit=fit, fit_used=nfit)
+    # warp and stabilize: case a's frames onto its reference with its transforms (frame 0 has none)
+    f, text = out['a_frames'][1:], out['a_text']
+    stab, union = stabilize(f, out['a_params'][1:], text)
+    out.update(stab_out=stab, stab_union=union)
+    # a thick text box (its middle more than 15 px from any pixel without text: the mean fills it)
+    thick = np.zeros_like(text)
+    thick[100:150, 60:200] = True
+    stab2, union2 = stabilize(f[:4], out['a_params'][1:5], thick)
+    out.update(stab2_text=thick, stab2_out=stab2, stab2_union=union2)
+    frame = out['b_frames'][3].astype(np.float32)
+    out.update(warp_params=np.array([3.3, -7.6, 0.012, -0.008]), warp_frame=frame)
+    out['warp_out'] = warp(frame, out['warp_params'])
+    out['warp_out_fill'] = warp(frame, out['warp_params'], fill=17.25)
     np.savez_compressed(os.path.join(HERE, 'stabilize.npz'), **out)
     print('wrote stabilize.npz', out['a_used'], out['b_used'], out['ncc_out'], fit, nfit)
 

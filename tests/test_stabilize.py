@@ -288,3 +288,95 @@ def test_coarse_track_big_transform():
     po, uo, no = oracle.coarse_track(f, 2, text, **kw)
     _same_transforms(p, po)
     assert np.array_equal(u, uo) and n == no and n >= 8
+
+
+# ---- stabilize.warp / stabilize.stabilize (stabilize.py:99-124) ----
+
+def test_oracle_warp_stabilize_golden():
+    o, u = oracle.stabilize(GOLD['a_frames'][1:], GOLD['a_params'][1:], GOLD['a_text'])
+    assert np.array_equal(o, GOLD['stab_out']) and np.array_equal(u, GOLD['stab_union'])
+    o, u = oracle.stabilize(GOLD['a_frames'][1:5], GOLD['a_params'][1:5], GOLD['stab2_text'])
+    assert np.array_equal(o, GOLD['stab2_out']) and np.array_equal(u, GOLD['stab2_union'])
+    assert np.array_equal(oracle.warp(GOLD['warp_frame'], GOLD['warp_params']), GOLD['warp_out'])
+    assert np.array_equal(oracle.warp(GOLD['warp_frame'], GOLD['warp_params'], 17.25), GOLD['warp_out_fill'])
+
+
+def test_oracle_box_mean_matches_definition():
+    """the box mean against a direct window average with the half-sample reflection (small case)"""
+    rng = np.random.default_rng(2)
+    x = rng.integers(0, 256, (13, 17)).astype(np.float32)
+    size = 5
+
+    def reflect(i, n):
+        i %= 2 * n
+        return i if i < n else 2 * n - 1 - i
+    a = np.array([[np.mean([x[reflect(r + k, 13), c] for k in range(-2, 3)]) for c in range(17)] for r in range(13)],
+                 np.float32)
+    b = np.array([[np.mean([a[r, reflect(c + k, 17)] for k in range(-2, 3)], dtype=np.float64) for c in range(17)]
+                  for r in range(13)]).astype(np.float32)
+    np.testing.assert_allclose(oracle.box_mean(x, size), b, rtol=1e-6)
+
+
+def _diff_stats(a, b):
+    d = np.abs(a.astype(np.int32) - b.astype(np.int32))
+    return int(d.max()) if d.size else 0, int((d > 0).sum())
+
+
+@pytest.mark.gpu
+def test_stabilize_golden():
+    """The GPU against the reference's own outputs: bit-identical frames and text union."""
+    from slipcam_b200 import stabilize
+    o, u = stabilize.stabilize(GOLD['a_frames'][1:], GOLD['a_params'][1:], GOLD['a_text'])
+    assert _diff_stats(o, GOLD['stab_out']) == (0, 0)
+    assert np.array_equal(u, GOLD['stab_union'])
+    o, u = stabilize.stabilize(GOLD['a_frames'][1:5], GOLD['a_params'][1:5], GOLD['stab2_text'])
+    assert _diff_stats(o, GOLD['stab2_out']) == (0, 0)
+    assert np.array_equal(u, GOLD['stab2_union'])
+
+
+@pytest.mark.gpu
+def test_warp_golden():
+    from slipcam_b200 import stabilize
+    np.testing.assert_array_equal(stabilize.warp(GOLD['warp_frame'], GOLD['warp_params']), GOLD['warp_out'])
+    np.testing.assert_array_equal(stabilize.warp(GOLD['warp_frame'], GOLD['warp_params'], fill=17.25),
+                                  GOLD['warp_out_fill'])
+
+
+@pytest.mark.gpu
+def test_stabilize_edges():
+    """no text at all; device frames; chunks; frames with NaN transforms (fill everywhere)"""
+    import torch
+    from slipcam_b200 import stabilize
+    f, p = GOLD['a_frames'][1:7], GOLD['a_params'][1:7].copy()
+    none = np.zeros_like(GOLD['a_text'])
+    o, u = stabilize.stabilize(f, p, none)
+    oo, uo = oracle.stabilize(f, p, none)
+    assert np.array_equal(o, oo) and not u.any() and not uo.any()
+    a = stabilize.stabilize(f, p, GOLD['a_text'])
+    b = stabilize.stabilize(torch.as_tensor(f).cuda(), torch.as_tensor(p), GOLD['a_text'])
+    c = stabilize.stabilize(f, p, GOLD['a_text'], chunk=4)
+    for other in (b, c):
+        assert np.array_equal(a[0], np.asarray(other[0].cpu() if hasattr(other[0], 'cpu') else other[0]))
+        assert np.array_equal(a[1], np.asarray(other[1].cpu() if hasattr(other[1], 'cpu') else other[1]))
+    p[2] = np.nan
+    o, u = stabilize.stabilize(f, p, GOLD['a_text'])
+    oo, uo = oracle.stabilize(f, p, GOLD['a_text'])
+    assert np.array_equal(o, oo) and np.array_equal(u, uo)
+
+
+@pytest.mark.gpu
+def test_stabilize_720p():
+    """720p frames with their true transforms: against the oracle, and the warped frames back on the
+    reference away from the text and the borders."""
+    from slipcam_b200 import stabilize, synth
+    boxes = ((900, 24, 1240, 68), (40, 650, 630, 700))
+    f, truth, text = synth.camera(4, 720, 1280, ref=0, seed=14, walk=(3.0, 3.0, 0.002, 0.002), text=boxes, noise=0.0)
+    o, u = stabilize.stabilize(f, truth, text)
+    oo, uo = oracle.stabilize(f, truth, text)
+    assert _diff_stats(o, oo) == (0, 0)
+    assert np.array_equal(u, uo)
+    inner = np.zeros((720, 1280), bool)
+    inner[80:600, 80:1200] = True
+    inner &= ~text
+    err = np.abs(o[1:].astype(np.int32) - f[0].astype(np.int32))[:, inner]
+    assert np.median(err) <= 1 and np.percentile(err, 99) <= 6
