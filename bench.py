@@ -142,6 +142,19 @@ def reference_cpu(frames, gross, down, across, nframes):
     return nframes * len(down) * len(across) / dt, dt, cores, kind
 
 
+def reference_cuda(workload='hd'):
+    """The reference's own CUDA backend (cuFFT) on this GPU, on the same workload through its own API
+    (host arrays, 64 frames): oracle/ref_cuda_bench.py in a process of its own."""
+    import subprocess
+    try:
+        r = subprocess.run([sys.executable, os.path.join(os.path.dirname(os.path.abspath(__file__)), 'oracle',
+                                                         'ref_cuda_bench.py'), '--workload', workload],
+                           capture_output=True, text=True, timeout=300)
+        return json.loads(r.stdout.strip().splitlines()[-1])
+    except Exception as e:   # a baseline only: its absence does not stop the line
+        return {'unavailable': f'{type(e).__name__}: {e}'[:200]}
+
+
 def run_reference(args):
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
@@ -341,6 +354,8 @@ def run_b200(args):
         if cpu is not None:
             out['cpu_baseline'] = {'value': cpu[0], 'unit': 'windows/s', 'cores': cpu[2], 'kind': cpu[3],
                                    'sample': f'{args.cpu_frames} frames of the same workload ({cpu[1]:.1f} s)'}
+        if world == 1 and not args.no_cpu:
+            out['reference_cuda'] = reference_cuda()
         print(json.dumps(out))
     if dist:
         dist.barrier()
@@ -472,6 +487,7 @@ def run_stream(args):
         'whole_job': {'value': n * nwin / job_s, 'unit': 'windows/s', 's': job_s,
                       'includes': 'Correlator creation, reference spectra (3.6 GB), the stream'},
         'valid_fraction': float(np.isfinite(r['offsets'][..., 0]).mean()),
+        'reference_cuda': reference_cuda('stream'),
     }))
 
 

@@ -45,7 +45,7 @@ def build():
     """Compile the oracle library (and the reference module when its sources are present)."""
     targets = ['oracle']
     if os.path.isdir('/root/reference/cxx'):
-        targets.append('ref')
+        targets += ['ref', 'ref_cuda']
     subprocess.run(['make', '-s', '-C', HERE, *targets], check=True)
 
 

@@ -145,8 +145,9 @@ def hd(n=300, h=720, w=1280, seed=1, device=None, count=None):
     return frames, motion, step, gross
 
 
-def stream(n=1000, h=1080, w=1920, seed=2, device=None):
-    """The 1080p streaming workload: frames, motion, step, gross (n, 2) int32."""
+def stream(n=1000, h=1080, w=1920, seed=2, device=None, count=None):
+    """The 1080p streaming workload: frames, motion, step, gross (n, 2) int32. count: render only the
+    first count frames (the motion of all n is the same either way)."""
     rng = np.random.default_rng(seed + 1000)
     t = np.arange(n) / 30.0
     walk = np.cumsum(rng.normal(0, 0.3, (n, 2)), 0)
@@ -154,7 +155,8 @@ def stream(n=1000, h=1080, w=1920, seed=2, device=None):
     motion = walk + shake
     k = np.arange(n)
     step = 60.0 * np.clip((k - n // 2) / 30.0, 0.0, 1.0)
-    frames = video(h, w, n, motion, step, sigma=2.0, noise=3.0, angle=30.0, seed=seed, device=device)
+    m = n if count is None else min(count, n)
+    frames = video(h, w, m, motion, step, sigma=2.0, noise=3.0, angle=30.0, seed=seed, device=device)
     return frames, motion, step, np.rint(motion).astype(np.int32)
 
 
