@@ -325,6 +325,10 @@ struct b200_handle {
     DevBuf<int64_t> d_sat2;
     DevBuf<float> d_dinv;
     Slot slot[2];
+    bool slots_ready = false;    // the slots are allocated (ensure_slots)
+    DevBuf<uint32_t> d_csat;     // coarse tracking: the second set of tables
+    DevBuf<int64_t> d_csat2;
+    DevBuf<float> d_cdinv;
     DevBuf<uint16_t> d_dtab;     // the FP16 DFT matrices of the tensor-core form
     DevBuf<int> d_status;        // device status word (3: a tensor-core wait gave up)
     DevBuf<CUtensorMap> d_tmaps; // TMA maps of the three denominator tables: slot 0, slot 1, device path
@@ -356,6 +360,33 @@ struct b200_handle {
     int64_t pixels() const { return int64_t(height) * width; }
     int dpitch() const { return (width + 3) & ~3; }                  // rows of 16-byte multiples
     int64_t dinv_size() const { return int64_t(height) * dpitch(); }
+
+    // the host path's two slots (device and page-locked host buffers, events, the TMA maps of their
+    // tables), allocated by the first host-path call: device-path callers never pay for them
+    void ensure_slots()
+    {
+        if (slots_ready) return;
+        const size_t G = size_t(group), P = G * nwin;
+        for (Slot &s : slot) {
+            s.frames.alloc(G * height * fpitch);
+            s.sat.alloc(G * sat_size());
+            s.sat2.alloc(G * sat_size());
+            s.dinv.alloc(G * dinv_size());
+            s.gross.alloc(2 * P);
+            s.out.alloc(7 * P);
+            s.hframes.alloc(G * height * fpitch);
+            s.hgross.alloc(2 * P);
+            s.hout.alloc(7 * P);
+            if (!s.in) CK(cudaEventCreateWithFlags(&s.in, cudaEventDisableTiming));
+            if (!s.done) CK(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+        }
+        if (tc_ok) {
+            const CUtensorMap maps[2] = {dinv_map(slot[0].dinv.p, height, width, dpitch(), int(G), M),
+                                         dinv_map(slot[1].dinv.p, height, width, dpitch(), int(G), M)};
+            CK(cudaMemcpy(d_tmaps.p, maps, sizeof(maps), cudaMemcpyHostToDevice));
+        }
+        slots_ready = true;
+    }
 
     // the tables and the correlation of nf frames (device memory) on stream s
     void run_group(const uint8_t *frames, int pitch, int nf, const int32_t *gross, int gross_mode,
@@ -657,29 +688,15 @@ int b200_create(const b200_params *p, int device, b200_handle **out)
             CK(cudaMemcpy(h->d_dtab.p, dt.data(), dt.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
         }
         if (N == kBigN) h->d_big.alloc(size_t(num_sms()) * big_scratch_per_cta(L, h->M));
-        const size_t G = size_t(h->group), P = G * h->nwin;
+        const size_t G = size_t(h->group);
         h->d_sat.alloc(G * h->sat_size());
         h->d_sat2.alloc(G * h->sat_size());
         h->d_dinv.alloc(G * h->dinv_size());
-        for (Slot &s : h->slot) {
-            s.frames.alloc(G * h->height * h->fpitch);
-            s.sat.alloc(G * h->sat_size());
-            s.sat2.alloc(G * h->sat_size());
-            s.dinv.alloc(G * h->dinv_size());
-            s.gross.alloc(2 * P);
-            s.out.alloc(7 * P);
-            s.hframes.alloc(G * h->height * h->fpitch);
-            s.hgross.alloc(2 * P);
-            s.hout.alloc(7 * P);
-            CK(cudaEventCreateWithFlags(&s.in, cudaEventDisableTiming));
-            CK(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
-        }
         if (h->tc_ok) {
-            const CUtensorMap maps[3] = {dinv_map(h->slot[0].dinv.p, h->height, h->width, h->dpitch(), int(G), h->M),
-                                         dinv_map(h->slot[1].dinv.p, h->height, h->width, h->dpitch(), int(G), h->M),
-                                         dinv_map(h->d_dinv.p, h->height, h->width, h->dpitch(), int(G), h->M)};
+            // the maps of the two slots are written when the slots are allocated
             h->d_tmaps.alloc(3);
-            CK(cudaMemcpy(h->d_tmaps.p, maps, sizeof(maps), cudaMemcpyHostToDevice));
+            const CUtensorMap m = dinv_map(h->d_dinv.p, h->height, h->width, h->dpitch(), int(G), h->M);
+            CK(cudaMemcpy(h->d_tmaps.p + 2, &m, sizeof(m), cudaMemcpyHostToDevice));
         }
         *out = h;
         g_create_error.clear();
@@ -752,6 +769,7 @@ int b200_correlate(b200_handle *h, const uint8_t *frames, int n, const int32_t *
         if (n == 0) return;
         if (!frames || !offset || !peak || !snr || !cov) fail(B200_EINVAL, "null input or output");
         CK(cudaSetDevice(h->device));
+        h->ensure_slots();
         const int G = h->group, nwin = h->nwin;
         const size_t frame_bytes = size_t(h->height) * h->width;
         const int ngroups = (n + G - 1) / G;
@@ -1101,9 +1119,15 @@ int b200_coarse_track_device(b200_handle *h, const uint8_t *frames, int n, int p
                    h->width, h->W, h->R, min_peak, prev, nullptr, nullptr};
         // two sets of tables: those of group g + 1 are built on the side stream while the frames of
         // group g are tracked on `stream` (the chain of one frame leaves most SMs idle)
-        uint32_t *sat[2] = {h->d_sat.p, h->slot[0].sat.p};
-        int64_t *sat2[2] = {h->d_sat2.p, h->slot[0].sat2.p};
-        float *dinv[2] = {h->d_dinv.p, h->slot[0].dinv.p};
+        if (!h->d_csat.p) {
+            const size_t G = size_t(h->group);
+            h->d_csat.alloc(G * h->sat_size());
+            h->d_csat2.alloc(G * h->sat_size());
+            h->d_cdinv.alloc(G * h->dinv_size());
+        }
+        uint32_t *sat[2] = {h->d_sat.p, h->d_csat.p};
+        int64_t *sat2[2] = {h->d_sat2.p, h->d_csat2.p};
+        float *dinv[2] = {h->d_dinv.p, h->d_cdinv.p};
         cudaEvent_t *ready = h->coarse_ev, *consumed = h->coarse_ev + 2, start = h->coarse_ev[4];
         cudaStream_t side = h->copy;
         const int G = h->group, groups = (n + G - 1) / G;

@@ -89,7 +89,7 @@ __device__ void block_sum(double (&x)[kTerms], double *red, double *tot)
 // of at least max(3 MAD, 0.3) pixels in either component; no fit below 4 windows), the frame's
 // transform (the previous one, and 0 windows, when there is no fit), then the next frame's gross
 // offsets: the rounded (half to even) position of each window under the transform, minus its
-// grid position. One CTA; shared memory: 6 nwin doubles and nwin bytes.
+// grid position. One CTA; shared memory: 8 nwin doubles and nwin bytes.
 __global__ void __launch_bounds__(kFitThreads) coarse_fit_kernel(FitArgs a)
 {
     extern __shared__ double smem[];
@@ -97,7 +97,8 @@ __global__ void __launch_bounds__(kFitThreads) coarse_fit_kernel(FitArgs a)
     double *d = smem;              // 2 nwin: dx of every window, then dy
     double *r = d + 2 * nwin;      // 2 nwin: the residuals of the current fit
     double *v = r + 2 * nwin;      // 2 nwin: the entries of a median (+inf: not in use)
-    uint8_t *use = reinterpret_cast<uint8_t *>(v + 2 * nwin);   // nwin
+    double *xy = v + 2 * nwin;     // 2 nwin: each window's centre relative to the image centre (X, then Y)
+    uint8_t *use = reinterpret_cast<uint8_t *>(xy + 2 * nwin);   // nwin
     __shared__ double red[kFitWarps * 14], tot[14], m[4], sel[2];
     __shared__ int s_count;
 
@@ -111,6 +112,8 @@ __global__ void __launch_bounds__(kFitThreads) coarse_fit_kernel(FitArgs a)
         const double oy = a.peaks[3 * k], ox = a.peaks[3 * k + 1], pk = a.peaks[3 * k + 2];
         const bool ok = a.keep[k] && inside && pk >= a.min_peak;
         use[k] = ok;
+        xy[k] = Xg - hw;
+        xy[nwin + k] = Yg - hh;
         // (x0 + search + half + ox) - w/2 - X0 with X0 = Xg - w/2, the reference's order
         d[k] = ok ? (double(x0 + a.search + half) + ox - hw) - (Xg - hw) : NAN;
         d[nwin + k] = ok ? (double(y0 + a.search + half) + oy - hh) - (Yg - hh) : NAN;
@@ -127,7 +130,7 @@ __global__ void __launch_bounds__(kFitThreads) coarse_fit_kernel(FitArgs a)
         double t[8] = {};
         for (int k = threadIdx.x; k < nwin; k += kFitThreads) {
             if (!use[k]) continue;
-            const double X = a.xc[k % a.nx] + a.coff - hw, Y = a.yc[k / a.nx] + a.coff - hh, dx = d[k], dy = d[nwin + k];
+            const double X = xy[k], Y = xy[nwin + k], dx = d[k], dy = d[nwin + k];
             t[0] += 1;
             t[1] += X;
             t[2] += Y;
@@ -157,7 +160,7 @@ __global__ void __launch_bounds__(kFitThreads) coarse_fit_kernel(FitArgs a)
         __syncthreads();
         // the residuals of the rows in use (NaN elsewhere); the median of the used ones
         for (int k = threadIdx.x; k < nwin; k += kFitThreads) {
-            const double X = a.xc[k % a.nx] + a.coff - hw, Y = a.yc[k / a.nx] + a.coff - hh;
+            const double X = xy[k], Y = xy[nwin + k];
             const bool u = use[k];
             r[k] = u ? d[k] - (m[0] - Y * m[2] + X * m[3]) : NAN;
             r[nwin + k] = u ? d[nwin + k] - (m[1] + X * m[2] + Y * m[3]) : NAN;
@@ -206,7 +209,7 @@ __global__ void __launch_bounds__(kFitThreads) coarse_fit_kernel(FitArgs a)
 
 }   // namespace
 
-size_t coarse_fit_smem(int nwin) { return size_t(6) * nwin * sizeof(double) + nwin; }
+size_t coarse_fit_smem(int nwin) { return size_t(8) * nwin * sizeof(double) + nwin; }
 
 cudaError_t launch_ncc_peaks(const float *surface, int n, int M, double *out, cudaStream_t s)
 {

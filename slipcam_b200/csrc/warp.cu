@@ -8,7 +8,8 @@
 //   window sums of these values are exact in double, so summing in any order gives scipy's bits.
 // * numpy's float32 mean: the pairwise sum (blocks of at most 128 values with 8 accumulators, split
 //   at n / 2 rounded down to a multiple of 8) divided by n in float32. The split depends only on n;
-//   the host builds the tree once and a CTA evaluates it level by level.
+//   the host builds the tree once; a thread sums each leaf, then a CTA per frame the tree, level by
+//   level.
 // * scipy.ndimage.map_coordinates(order=1, mode='constant'): a coordinate outside [0, n - 1] takes
 //   cval; inside, the bilinear weights in double; the result rounded to float32.
 //
@@ -126,30 +127,38 @@ __device__ __forceinline__ float leaf_sum(const Get &get, int64_t start, int n)
     return res;
 }
 
-constexpr int kMeanThreads = 1024;
+constexpr int kLeafThreads = 128;
+constexpr int kTreeThreads = 1024;
 
-// numpy's float32 mean of frame b's values x[gather[i]] (gather may be null: x[i]), i < plan.n:
-// the leaves in parallel, then the tree level by level; vals: per frame leaves + internal floats
-__global__ void __launch_bounds__(kMeanThreads) pairwise_mean_kernel(const float *__restrict__ x, int64_t fstride,
-                                                                    const int32_t *__restrict__ gather, PlanDev p,
-                                                                    float *__restrict__ vals, float *__restrict__ mean)
+// numpy's pairwise sums of the leaves of frame b's values x[gather[i]] (gather may be null: x[i]),
+// one thread per leaf; grid (leaves / 128, frames). vals: per frame leaves + internal floats
+__global__ void __launch_bounds__(kLeafThreads) pairwise_leaves_kernel(const float *__restrict__ x, int64_t fstride,
+                                                                      const int32_t *__restrict__ gather, PlanDev p,
+                                                                      float *__restrict__ vals)
 {
-    const int b = blockIdx.x;
+    const int l = blockIdx.x * kLeafThreads + threadIdx.x, b = blockIdx.y;
+    if (l >= p.leaves) return;
     const float *xb = x + b * fstride;
     float *v = vals + size_t(b) * (p.leaves + p.internal);
+    if (gather)
+        v[l] = leaf_sum([&](int64_t i) { return xb[gather[i]]; }, p.leaf_start[l], p.leaf_len[l]);
+    else
+        v[l] = leaf_sum([&](int64_t i) { return xb[i]; }, p.leaf_start[l], p.leaf_len[l]);
+}
+
+// the tree over frame b's leaf sums, level by level, then the mean: sum / n in float32 (NaN for no
+// values, as numpy). One CTA per frame.
+__global__ void __launch_bounds__(kTreeThreads) pairwise_tree_kernel(PlanDev p, float *__restrict__ vals,
+                                                                    float *__restrict__ mean)
+{
+    const int b = blockIdx.x;
+    float *v = vals + size_t(b) * (p.leaves + p.internal);
     if (p.n == 0) {
-        if (threadIdx.x == 0) mean[b] = NAN;   // numpy: the mean of nothing
+        if (threadIdx.x == 0) mean[b] = NAN;
         return;
     }
-    for (int l = threadIdx.x; l < p.leaves; l += kMeanThreads) {
-        if (gather)
-            v[l] = leaf_sum([&](int64_t i) { return xb[gather[i]]; }, p.leaf_start[l], p.leaf_len[l]);
-        else
-            v[l] = leaf_sum([&](int64_t i) { return xb[i]; }, p.leaf_start[l], p.leaf_len[l]);
-    }
-    __syncthreads();
     for (int h = 1; h < p.levels; ++h) {
-        for (int i = p.level_off[h - 1] + threadIdx.x; i < p.level_off[h]; i += kMeanThreads)
+        for (int i = p.level_off[h - 1] + threadIdx.x; i < p.level_off[h]; i += kTreeThreads)
             v[p.leaves + i] = __fadd_rn(v[p.left[i]], v[p.right[i]]);
         __syncthreads();
     }
@@ -157,6 +166,16 @@ __global__ void __launch_bounds__(kMeanThreads) pairwise_mean_kernel(const float
         const float total = p.internal ? v[p.leaves + p.internal - 1] : v[0];
         mean[b] = __fdiv_rn(total, float(p.n));
     }
+}
+
+// numpy's float32 mean of nb frames (the leaves, then the trees) on stream st
+void pairwise_mean(const float *x, int64_t fstride, const int32_t *gather, const PlanDev &p, float *vals, float *mean,
+                   unsigned nb, cudaStream_t st)
+{
+    if (p.leaves > 0)
+        pairwise_leaves_kernel<<<dim3(unsigned((p.leaves + kLeafThreads - 1) / kLeafThreads), nb), kLeafThreads, 0, st>>>(
+            x, fstride, gather, p, vals);
+    pairwise_tree_kernel<<<nb, kTreeThreads, 0, st>>>(p, vals, mean);
 }
 
 // --------------------------------------------------------------------------------------------
@@ -186,7 +205,7 @@ __global__ void box_cols_kernel(const uint8_t *__restrict__ frames, int64_t fstr
     if (c >= w || r0 >= h) return;
     const uint8_t *f = frames ? frames + b * fstride : nullptr;
     auto in = [&](int r) -> int {
-        const int rr = reflect_line(r, h);
+        const int rr = (r >= 0 && r < h) ? r : reflect_line(r, h);
         const int t = text ? text[size_t(rr) * w + c] : 0;
         return f ? (t ? 0 : int(f[int64_t(rr) * pitch + c])) : (1 - t);
     };
@@ -221,8 +240,11 @@ __global__ void __launch_bounds__(128) box_rows_kernel(const float *__restrict__
     if (r0 >= h) return;   // the whole warp: no barrier below is CTA-wide
     const int s1 = size / 2;
     const float *x = in + size_t(b) * h * w;
-    for (int i = 0; i < kRowTile && r0 + i < h; ++i)
-        for (int j = lane; j < span; j += 32) tile[i * pitch_s + j] = x[size_t(r0 + i) * w + reflect_line(c0 - s1 + j, w)];
+    const bool interior = c0 - s1 >= 0 && c0 - s1 + span <= w;
+    for (int i = 0; i < kRowTile && r0 + i < h; ++i) {
+        const float *xr = x + size_t(r0 + i) * w;
+        for (int j = lane; j < span; j += 32) tile[i * pitch_s + j] = xr[interior ? c0 - s1 + j : reflect_line(c0 - s1 + j, w)];
+    }
     __syncwarp();
     if (r0 + lane < h) {
         const float *row = tile + lane * pitch_s;
@@ -481,8 +503,7 @@ int b200_stab_frames_device(b200_stab *s, const uint8_t *frames, int n, int pitc
                 // the text blanked with the local mean of the pixels around it (stabilize.py:118-121):
                 // the mean of the pixels without text, from the float32 frame
                 to_float_kernel<<<dim3(pblocks, nb), 256, 0, st>>>(fr, fstride, pitch, h, w, s->d_blank);
-                pairwise_mean_kernel<<<nb, kMeanThreads, 0, st>>>(s->d_blank, px, s->d_keep_idx, s->plan_keep, s->d_vals,
-                                                                  mean_keep);
+                pairwise_mean(s->d_blank, px, s->d_keep_idx, s->plan_keep, s->d_vals, mean_keep, nb, st);
                 box_cols_kernel<<<dim3(unsigned((w + 127) / 128), unsigned((h + kColSeg - 1) / kColSeg), nb), 128, 0, st>>>(
                     fr, fstride, pitch, s->d_text, h, w, s->size, s->d_work);
                 box_rows_kernel<<<dim3(unsigned((h + 127) / 128), unsigned((w + kRowTile - 1) / kRowTile), nb), 128,
@@ -492,7 +513,7 @@ int b200_stab_frames_device(b200_stab *s, const uint8_t *frames, int n, int pitc
                 to_float_kernel<<<dim3(pblocks, nb), 256, 0, st>>>(fr, fstride, pitch, h, w, s->d_blank);
             }
             // the fill: the mean of the blanked frame (warp's default, stabilize.py:105)
-            pairwise_mean_kernel<<<nb, kMeanThreads, 0, st>>>(s->d_blank, px, nullptr, s->plan_all, s->d_vals, mean_blank);
+            pairwise_mean(s->d_blank, px, nullptr, s->plan_all, s->d_vals, mean_blank, nb, st);
             warp_kernel<<<dim3(pblocks, nb), 256, 0, st>>>(s->d_blank, h, w, params + 4 * size_t(f0), mean_blank, 0.0f,
                                                           union_mask ? s->d_text : nullptr, out + f0 * px, px, nullptr,
                                                           union_mask);

@@ -16,8 +16,8 @@ stream-ordered steps on the GPU and no host round trip:
 The frame loop runs in the library (b200_coarse_track_device): per group of frames the tables in one
 batch, then three launches per frame.
 
-Frames in host memory are staged through two page-locked buffers and copied on a side stream while
-the previous chunk is tracked; CUDA tensors are read in place.
+Frames in host memory are copied from the caller's array on a side stream while the previous chunk
+is tracked; CUDA tensors are read in place.
 
 The resampling half of the module, warp and stabilize (stabilize.py:99-124), runs on the GPU too
 (csrc/warp.cu): the text blanked with scipy's box means, the frames warped with map_coordinates'
@@ -77,6 +77,15 @@ def _keep(ref, text, yc, xc, half):
             keep[i, j] = (not text[y - half:y + half, x - half:x + half].any()
                           and refimg[y - half:y + half, x - half:x + half].std() > 2)
     return keep
+
+
+def _host_range(frames, lo, hi):
+    """frames[lo:hi] as a C-contiguous, writable numpy array (a copy only when it is not one already:
+    memory-mapped, strided or read-only input)"""
+    src = frames[lo:hi]
+    if not (isinstance(src, np.ndarray) and src.flags.c_contiguous and src.flags.writeable):
+        src = np.array(src, np.uint8, order='C')
+    return src
 
 
 def _runs(order, chunk):
@@ -163,25 +172,25 @@ class CoarseTracker:
                             track(rev.data_ptr(), len(run), at, c == 0)
                         at += len(run)
             elif order:
+                # each chunk copied straight from the caller's array on a side stream (a backward
+                # chunk reversed on the device), the copy of chunk k + 1 overlapping the tracking of
+                # chunk k; two device buffers, each reused once its chunk is tracked
                 C = min(chunk, len(order))
-                host = [torch.empty((C, h, w), dtype=torch.uint8, pin_memory=True) for _ in range(2)]
                 devb = [torch.empty((C, h, w), dtype=torch.uint8, device=dev) for _ in range(2)]
                 copy = torch.cuda.Stream(dev)
                 done = [None, None]
                 b = 0
                 for frames_in_order in passes:
                     for c, run in enumerate(_runs(frames_in_order, C)):
-                        if done[b] is not None:
-                            done[b].synchronize()   # the chunk before last is tracked: both buffers b are free
-                        dst = host[b].numpy()[:len(run)]
-                        if run[0] <= run[-1]:
-                            np.copyto(dst, frames[run[0]:run[-1] + 1])
-                        elif run[-1] > 0:
-                            np.copyto(dst, frames[run[0]:run[-1] - 1:-1])
-                        else:
-                            np.copyto(dst, frames[run])
+                        lo, hi = min(run[0], run[-1]), max(run[0], run[-1]) + 1
+                        src = torch.from_numpy(_host_range(frames, lo, hi))
                         with torch.cuda.stream(copy):
-                            devb[b][:len(run)].copy_(host[b][:len(run)], non_blocking=True)
+                            if done[b] is not None:
+                                copy.wait_event(done[b])   # the chunk before last is tracked
+                            if run[0] <= run[-1]:
+                                devb[b][:len(run)].copy_(src, non_blocking=True)
+                            else:
+                                devb[b][:len(run)].copy_(src.to(dev, non_blocking=True).flip(0))
                             ready = copy.record_event()
                         stream.wait_event(ready)
                         track(devb[b].data_ptr(), len(run), at, c == 0)
@@ -272,10 +281,11 @@ class Stabilizer:
         if ctx and _lib is not None and _lib._lib is not None:
             _lib._lib.b200_stab_destroy(ctx)
 
-    def run(self, frames, params, chunk=64):
+    def run(self, frames, params, chunk=16):
         """(frames warped onto the reference, uint8, with their text blanked; the union of the warped
         text masks, bool) for frames (n x height x width uint8, numpy or CUDA tensor) and params
-        (n x 4: p, q, a, s). Numpy in, numpy out; a CUDA tensor in, CUDA tensors out."""
+        (n x 4: p, q, a, s). Numpy in, numpy out; a CUDA tensor in, CUDA tensors out. chunk: frames
+        per host-to-device copy."""
         import torch
         n, h, w = frames.shape
         if (h, w) != (self.height, self.width):
@@ -301,24 +311,44 @@ class Stabilizer:
                 if n:
                     run(f, n, 0, out)
                 return out, union.bool()
+            # two sets of device buffers; chunk k + 1 is copied in (straight from the caller's array,
+            # on a side stream) and warped while chunk k is copied out into the result (on another)
             out = np.empty((n, h, w), np.uint8)
             C = max(1, min(chunk, n))
-            host_in = torch.empty((C, h, w), dtype=torch.uint8, pin_memory=True)
-            host_out = torch.empty((C, h, w), dtype=torch.uint8, pin_memory=True)
-            dev_in = torch.empty((C, h, w), dtype=torch.uint8, device=dev)
-            dev_out = torch.empty((C, h, w), dtype=torch.uint8, device=dev)
-            for k0 in range(0, n, C):
-                m = min(C, n - k0)
-                np.copyto(host_in.numpy()[:m], frames[k0:k0 + m])
-                dev_in[:m].copy_(host_in[:m], non_blocking=True)
-                run(dev_in, m, k0, dev_out)
-                host_out[:m].copy_(dev_out[:m], non_blocking=True)
-                stream.synchronize()
-                out[k0:k0 + m] = host_out.numpy()[:m]
+            dev_in = [torch.empty((C, h, w), dtype=torch.uint8, device=dev) for _ in range(2)]
+            dev_out = [torch.empty((C, h, w), dtype=torch.uint8, device=dev) for _ in range(2)]
+            copy_in, copy_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+            chunks = [(k0, min(C, n - k0)) for k0 in range(0, n, C)]
+            done = [None, None]
+
+            def start(c):
+                b, (k0, m) = c % 2, chunks[c]
+                src = torch.from_numpy(_host_range(frames, k0, k0 + m))
+                with torch.cuda.stream(copy_in):
+                    if done[b] is not None:
+                        copy_in.wait_event(done[b])   # chunk c - 2 no longer reads dev_in[b]
+                    dev_in[b][:m].copy_(src, non_blocking=True)
+                    ready = copy_in.record_event()
+                stream.wait_event(ready)
+                run(dev_in[b], m, k0, dev_out[b])
+                done[b] = stream.record_event()
+
+            def finish(c):
+                b, (k0, m) = c % 2, chunks[c]
+                with torch.cuda.stream(copy_out):
+                    copy_out.wait_event(done[b])
+                    torch.from_numpy(out[k0:k0 + m]).copy_(dev_out[b][:m])   # returns when copied
+            if chunks:
+                start(0)
+            for c in range(1, len(chunks)):
+                start(c)
+                finish(c - 1)
+            if chunks:
+                finish(len(chunks) - 1)
             return out, union.cpu().numpy().astype(bool)
 
 
-def stabilize(frames, params, text, *, chunk=64):
+def stabilize(frames, params, text, *, chunk=16):
     """The frames warped onto the reference (uint8), with their text blanked (the local mean), and the
     union of the warped text masks (stabilize.py:109-124). frames: n x height x width uint8 (numpy or
     CUDA tensor); params: n x 4 (coarse_track's transforms); text: height x width bool."""
