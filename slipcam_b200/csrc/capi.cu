@@ -474,6 +474,9 @@ struct b200_handle {
             B200_DISPATCH_TC(N, launch_corr_tc, a, dt, d_status.p, dm, s);
         } else if (N == kBigN) {
             launch_corr_big(a, d_big.p, s);
+        } else if (N == 192) {
+            // one 154 KB tile per SM: 512 threads per pair keep 16 warps resident instead of 8
+            launch_corr_latency<192>(a, s);
         } else {
             B200_DISPATCH(N, launch_corr, a, s);
         }
