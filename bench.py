@@ -194,6 +194,26 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def shard_starts(rank, world, nframes, batch, count):
+    """The first frames of the `count` batches that rank takes from a video of nframes frames (frame 0
+    the reference): batch b (frames 1 + b batch ...) goes to rank b % world, so the ranks' batches
+    are disjoint until the video is used up, then they wrap around. No data crosses ranks."""
+    nb = (nframes - 1) // batch
+    if nb < 1:
+        raise ValueError('the video holds no full batch')
+    return [1 + ((rank + world * i) % nb) * batch for i in range(count)]
+
+
+def max_over_ranks(x, dist, device):
+    """x's maximum over the ranks (the slowest rank's time); x itself with one rank"""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_b200(args):
     import torch
     rank = int(os.environ.get('RANK', '0'))
@@ -217,8 +237,7 @@ def run_b200(args):
     cor.set_reference(frames[0])
     fft_n = cor.info()[2]
     BATCH = args.batch
-    nb = (len(frames) - 1) // BATCH
-    starts = [1 + ((rank + world * i) % nb) * BATCH for i in range(args.warmup + args.steps + 8)]
+    starts = shard_starts(rank, world, len(frames), BATCH, args.warmup + args.steps + 8)
 
     def step_dev(i):
         s = starts[i]
@@ -248,10 +267,7 @@ def run_b200(args):
     kernel_ms, kernel_launches, pairs = cor.profile_read()
     cor.profile(False)
     launches = cor.info()[3] - launches0
-    if dist:
-        t = torch.tensor([ms], device='cuda')
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, 'cuda')
     value = world * args.steps * BATCH * nwin / (ms / 1e3)
 
     # the other form on the same steps (device time), for comparison
@@ -286,10 +302,7 @@ def run_b200(args):
         s = starts[args.warmup + i]
         r = cor.correlate(host_np[s:s + BATCH], gross=gross[s:s + BATCH])
     e2e_s = time.perf_counter() - t
-    if dist:
-        tt = torch.tensor([e2e_s], device='cuda')
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = max_over_ranks(e2e_s, dist, 'cuda')
     e2e = world * args.steps * BATCH * nwin / e2e_s
 
     # accuracy on one batch: offsets against the FP64 oracle on a sub-grid of windows
