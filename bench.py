@@ -578,12 +578,14 @@ def run_stabilize(args):
         p, u, c = tr.run(frames, 0)
     torch.cuda.synchronize()
     steps = max(1, min(args.steps, 10))
+    launches0 = tr._cor.info()[3]
     e0.record()
     for _ in range(steps):
         p, u, c = tr.run(frames, 0)
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
+    launches = (tr._cor.info()[3] - launches0) // steps
     def e2e_time(call):   # after a warm-up call, the median of three timed calls
         call()
         times = []
@@ -625,7 +627,7 @@ def run_stabilize(args):
         'e2e': {'value': (n - 1) / e2e_s, 'unit': 'frames/s', 'h2d_bytes_per_step': (n - 1) * 720 * 1280,
                 'd2h_bytes_per_step': (n - 1) * 36,
                 'path': 'stabilize.coarse_track over a host array (templates built per call), median of 3 calls'},
-        'gpu_launches': 3 * (n - 1) + 3 * ((n - 1 + 31) // 32),
+        'gpu_launches': launches,
         'cpu_baseline': {'value': cpu_frames / cpu_s, 'unit': 'frames/s', 'cores': 1, 'kind': 'port',
                          'sample': f'{cpu_frames} frames of the same video ({cpu_s:.1f} s)'},
         'agreement': {'vs_oracle_max_px': float(np.abs(po[1:] - p[1:cpu_frames + 1])[:, :2].max()),

@@ -1158,15 +1158,16 @@ int b200_coarse_track_device(b200_handle *h, const uint8_t *frames, int n, int p
                     a.ncc = h->d_cpeaks.p;
                     B200_DISPATCH(h->N, launch_corr_latency, a, s);
                     CK(cudaGetLastError());
+                    h->launches += 1;
                 } else {
-                    h->run_corr_tail(a, 1, a.dinv, B200_FORM_FFT32, s);
+                    h->run_corr_tail(a, 1, a.dinv, B200_FORM_FFT32, s);   // counts its launch
                     CK(launch_ncc_peaks(surf, int(nwin), h->M, h->d_cpeaks.p, s));
                     h->launches += 1;
                 }
                 fa.params = params + 4 * size_t(f);
                 fa.used = used + f;
                 CK(launch_coarse_fit(fa, s));
-                h->launches += 2;
+                h->launches += 1;
             }
             CK(cudaEventRecord(consumed[g % 2], s));
         }
