@@ -19,7 +19,7 @@ namespace b200 {
 namespace {
 
 constexpr int kPeakThreads = 256;
-constexpr int kFitThreads = 256;
+constexpr int kFitThreads = 512;
 constexpr int kFitWarps = kFitThreads / 32;
 constexpr int kGrossLimit = 1 << 29;   // a predicted position beyond this is outside every frame
 
@@ -38,30 +38,78 @@ __device__ __forceinline__ void similarity(const double *m, double x, double y, 
     yo = __dadd_rn(__dadd_rn(__dadd_rn(y, m[1]), __dmul_rn(m[2], x)), __dmul_rn(m[3], y));
 }
 
-// numpy.median of the n finite entries of v[0, m) (the others +inf): each entry's rank among them
-// (ties broken by position), the entries of the middle rank(s) picked. O(m^2 / threads) compares,
-// which for the few thousand entries of a grid is less work than a sort's barriers. sel: 2 doubles.
-__device__ double median_by_rank(const double *v, int m, int n, double *sel)
+// the n finite entries of v[0, m) (the others +inf) in ascending order into srt[0, n): each entry's
+// rank among them (ties broken by position) counted by up to kFitThreads / m threads, each over a
+// slice of the entries, then the entries scattered to their ranks. rank: m ints of shared memory.
+__device__ void sort_by_rank(const double *v, int m, double *srt, int *rank)
 {
-    const int lo = (n - 1) / 2, hi = n / 2;
-    if (threadIdx.x < 2) sel[threadIdx.x] = NAN;
+    const int S = max(1, kFitThreads / m);
+    for (int i = threadIdx.x; i < m; i += kFitThreads) rank[i] = 0;
     __syncthreads();
-    for (int i = threadIdx.x; i < m; i += kFitThreads) {
-        const double x = v[i];
-        if (!(x < INFINITY)) continue;
-        int rank = 0;
+    if (S > 1) {
+        const int i = threadIdx.x % m, sl = threadIdx.x / m;
+        if (threadIdx.x < S * m) {
+            const double x = v[i];
+            if (x < INFINITY) {
+                const int j0 = sl * m / S, j1 = (sl + 1) * m / S;
+                int r = 0;
 #pragma unroll 8
-        for (int j = 0; j < m; ++j) {
-            const double y = v[j];
-            rank += (y < x) | ((y == x) & (j < i));
+                for (int j = j0; j < j1; ++j) {
+                    const double y = v[j];
+                    r += (y < x) | ((y == x) & (j < i));
+                }
+                atomicAdd(rank + i, r);
+            }
         }
-        if (rank == lo) sel[0] = x;
-        if (rank == hi) sel[1] = x;
+    } else {
+        for (int i = threadIdx.x; i < m; i += kFitThreads) {
+            const double x = v[i];
+            if (!(x < INFINITY)) continue;
+            int r = 0;
+#pragma unroll 8
+            for (int j = 0; j < m; ++j) {
+                const double y = v[j];
+                r += (y < x) | ((y == x) & (j < i));
+            }
+            rank[i] = r;
+        }
     }
     __syncthreads();
-    const double med = n % 2 ? sel[1] : (sel[0] + sel[1]) / 2;
+    for (int i = threadIdx.x; i < m; i += kFitThreads)
+        if (v[i] < INFINITY) srt[rank[i]] = v[i];
     __syncthreads();
-    return med;
+}
+
+// numpy.median(|s - med|) of the n ascending values srt (med their median): the k + 1 values closest
+// to med are consecutive in srt, so the k-th smallest deviation is the least, over the windows of
+// k + 1 consecutive values, of the larger deviation at the window's two ends. The two middle ranks
+// in one reduction over the windows.
+__device__ double median_abs_dev(const double *srt, int n, double med, double *red2)
+{
+    const int k1 = (n - 1) / 2, k2 = n / 2;
+    double b1 = INFINITY, b2 = INFINITY;
+    for (int a0 = threadIdx.x; a0 < n; a0 += kFitThreads) {
+        const double lo = fabs(srt[a0] - med);
+        if (a0 + k1 < n) b1 = fmin(b1, fmax(lo, fabs(srt[a0 + k1] - med)));
+        if (a0 + k2 < n) b2 = fmin(b2, fmax(lo, fabs(srt[a0 + k2] - med)));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        b1 = fmin(b1, __shfl_xor_sync(0xffffffffu, b1, o));
+        b2 = fmin(b2, __shfl_xor_sync(0xffffffffu, b2, o));
+    }
+    const int warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        red2[2 * warp] = b1;
+        red2[2 * warp + 1] = b2;
+    }
+    __syncthreads();
+    double d1 = INFINITY, d2 = INFINITY;
+    for (int w = 0; w < kFitWarps; ++w) {
+        d1 = fmin(d1, red2[2 * w]);
+        d2 = fmin(d2, red2[2 * w + 1]);
+    }
+    __syncthreads();
+    return n % 2 ? d2 : (d1 + d2) / 2;
 }
 
 // sum over the CTA of kTerms doubles per thread, the same order on every run; the totals land in tot
@@ -89,7 +137,7 @@ __device__ void block_sum(double (&x)[kTerms], double *red, double *tot)
 // of at least max(3 MAD, 0.3) pixels in either component; no fit below 4 windows), the frame's
 // transform (the previous one, and 0 windows, when there is no fit), then the next frame's gross
 // offsets: the rounded (half to even) position of each window under the transform, minus its
-// grid position. One CTA; shared memory: 8 nwin doubles and nwin bytes.
+// grid position. One CTA; shared memory: 10 nwin doubles, 2 nwin ints and nwin bytes.
 __global__ void __launch_bounds__(kFitThreads) coarse_fit_kernel(FitArgs a)
 {
     extern __shared__ double smem[];
@@ -98,8 +146,10 @@ __global__ void __launch_bounds__(kFitThreads) coarse_fit_kernel(FitArgs a)
     double *r = d + 2 * nwin;      // 2 nwin: the residuals of the current fit
     double *v = r + 2 * nwin;      // 2 nwin: the entries of a median (+inf: not in use)
     double *xy = v + 2 * nwin;     // 2 nwin: each window's centre relative to the image centre (X, then Y)
-    uint8_t *use = reinterpret_cast<uint8_t *>(xy + 2 * nwin);   // nwin
-    __shared__ double red[kFitWarps * 14], tot[14], m[4], sel[2];
+    double *srt = xy + 2 * nwin;   // 2 nwin: the residuals in use, ascending
+    int *rank = reinterpret_cast<int *>(srt + 2 * nwin);        // 2 nwin
+    uint8_t *use = reinterpret_cast<uint8_t *>(rank + 2 * nwin);   // nwin
+    __shared__ double red[kFitWarps * 14], tot[14], m[4];
     __shared__ int s_count;
 
     const double hw = a.width / 2.0, hh = a.height / 2.0;
@@ -168,9 +218,9 @@ __global__ void __launch_bounds__(kFitThreads) coarse_fit_kernel(FitArgs a)
         __syncthreads();
         const int n = 2 * s_count;
         for (int i = threadIdx.x; i < 2 * nwin; i += kFitThreads) v[i] = use[i % nwin] ? r[i] : INFINITY;
-        const double med = median_by_rank(v, 2 * nwin, n, sel);
-        for (int i = threadIdx.x; i < 2 * nwin; i += kFitThreads) v[i] = use[i % nwin] ? fabs(r[i] - med) : INFINITY;
-        const double mad = 1.4826 * median_by_rank(v, 2 * nwin, n, sel);
+        sort_by_rank(v, 2 * nwin, srt, rank);
+        const double med = n % 2 ? srt[n / 2] : (srt[n / 2 - 1] + srt[n / 2]) / 2;   // numpy.median
+        const double mad = 1.4826 * median_abs_dev(srt, n, med, red);
         const double thr = fmax(3 * mad, 0.3);
         for (int k = threadIdx.x; k < nwin; k += kFitThreads)
             use[k] = use[k] && fabs(r[k]) < thr && fabs(r[nwin + k]) < thr;
@@ -207,9 +257,10 @@ __global__ void __launch_bounds__(kFitThreads) coarse_fit_kernel(FitArgs a)
     }
 }
 
+
 }   // namespace
 
-size_t coarse_fit_smem(int nwin) { return size_t(8) * nwin * sizeof(double) + nwin; }
+size_t coarse_fit_smem(int nwin) { return size_t(10) * nwin * sizeof(double) + size_t(2) * nwin * sizeof(int) + nwin; }
 
 cudaError_t launch_ncc_peaks(const float *surface, int n, int M, double *out, cudaStream_t s)
 {
