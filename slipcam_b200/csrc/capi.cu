@@ -171,17 +171,39 @@ void prepare_big()
     CK(cudaGetDevice(&dev));
     if (dev >= 0 && dev < 64 && done[dev]) return;
     const int smem = int(BigGeo<kBigN>::smem_bytes);
-    CK(cudaFuncSetAttribute(corr_big_kernel<kBigN, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CK(cudaFuncSetAttribute(corr_big_cluster_kernel<kBigN, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            int(BigClusterGeo<kBigN>::smem_bytes)));
     CK(cudaFuncSetAttribute(spectra_big_kernel<kBigN, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     if (dev >= 0 && dev < 64) done[dev] = true;
 }
 
-void launch_corr_big(const CorrArgs &a, float2 *scratch, cudaStream_t s)
+// the two-CTA clusters of the big transform that fit on the device at once (its persistent grid)
+int big_clusters()
+{
+    static int cached[64] = {};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && cached[dev]) return cached[dev];
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(unsigned(num_sms() / 2 * 2), 1, 1);
+    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.dynamicSmemBytes = BigClusterGeo<kBigN>::smem_bytes;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, corr_big_cluster_kernel<kBigN, kThreads>, &cfg) != cudaSuccess || n < 1) {
+        cudaGetLastError();
+        n = num_sms() / 2;
+    }
+    if (dev >= 0 && dev < 64) cached[dev] = n;
+    return n;
+}
+
+// the correlation of the big transform: two-CTA clusters holding the half spectrum in their
+// shared memories (the per-CTA scratch serves the reference spectra only)
+void launch_corr_big(const CorrArgs &a, float2 *, cudaStream_t s)
 {
     prepare_big();
-    const int grid = std::min(a.nwin * a.nf, num_sms());
-    corr_big_kernel<kBigN, kThreads><<<unsigned(grid), kThreads, BigGeo<kBigN>::smem_bytes, s>>>(
-        a, scratch, big_scratch_per_cta(a.L, a.M));
+    const int clusters = std::min(a.nwin * a.nf, big_clusters());
+    corr_big_cluster_kernel<kBigN, kThreads><<<unsigned(2 * clusters), kThreads, BigClusterGeo<kBigN>::smem_bytes, s>>>(a);
 }
 
 // cuTensorMapEncodeTiled, from the driver through the runtime (no link against libcuda)

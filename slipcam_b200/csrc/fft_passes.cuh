@@ -210,12 +210,14 @@ B200_HD void col_pass(const Ex &ex, float2 *S, int Lr, int M, const float2 *TW, 
 }
 
 // The inverse row pass: rows [0, M) of S hold column-inverted half spectra; on return row u holds
-// norm(u, c, value) for c in [0, M) as floats (pitch RP), value the unnormalized correlation.
+// norm(u, c, value) for c in [0, cols) as floats (pitch RP), value the unnormalized correlation;
+// cols defaults to M (a square surface; a caller with part of its rows passes the surface width).
 template <int N, class Ex, class Norm>
-B200_HD void row_inverse(const Ex &ex, float2 *S, int M, const float2 *TWI, Norm &&norm)
+B200_HD void row_inverse(const Ex &ex, float2 *S, int M, const float2 *TWI, Norm &&norm, int cols = -1)
 {
     using G = Geo<N>;
     constexpr int N2 = G::N2, NHP = G::NHP;
+    const int C = cols < 0 ? M : cols;
     struct St {
         float2 z[N2];
         float2 y[16];
@@ -262,7 +264,7 @@ B200_HD void row_inverse(const Ex &ex, float2 *S, int M, const float2 *TWI, Norm
 #pragma unroll
                         for (int n1 = 0; n1 < 16; ++n1) {
                             const int c = N2 * n1 + n2;
-                            if (c < M) {
+                            if (c < C) {
                                 Sr[size_t(u1) * G::RP + c] = norm(u1, c, s.y[n1].x);
                                 if (u2 < M) Sr[size_t(u2) * G::RP + c] = norm(u2, c, s.y[n1].y);
                             }
