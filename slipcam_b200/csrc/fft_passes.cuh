@@ -56,6 +56,14 @@ struct HostExec {
     }
 };
 
+// The row pairs a warp takes at once in the row passes: lanes 0-15 take pair_of(g, 0), lanes 16-31
+// pair_of(g, 1), two pairs apart. Each half-warp then holds one pair, so its 8-byte accesses (16
+// distinct slots of a row) meet no bank twice, and the two pairs' rows are 4 NHP complex values
+// apart, 16 banks for NHP twice an odd number, so the warp's 4-byte reads of the two pairs do not
+// overlap either. Items g < pair_items(P) cover the pairs 0 .. P - 1 (the rest idle).
+B200_HD int pair_of(int g, int half) { return 4 * (g >> 1) + (g & 1) + 2 * half; }
+B200_HD int pair_items(int P) { return 2 * ((P + 3) / 4); }
+
 // rows [0, 2P) of S hold real rows (floats, pitch RP, element n of a row at float column
 // off + n, off < 4); on return, their half spectra
 template <int N, class Ex>
@@ -69,10 +77,10 @@ B200_HD void row_forward(const Ex &ex, float2 *S, int P, const float2 *TW, int o
         float2 a[NU], b[NU];
     };
     ex.for_warps([&](int warp) {
-        for (int g = warp; 2 * g < P; g += ex.nwarps()) {
+        for (int g = warp; g < pair_items(P); g += ex.nwarps()) {
             ex.template run<St>(
                 [&](int lane, St &s) {   // step 1 on the complex row (row 2p) + i (row 2p+1)
-                    const int p = 2 * g + (lane & 1), n2 = lane >> 1;
+                    const int p = pair_of(g, lane >> 4), n2 = lane & 15;
                     if (p < P && n2 < N2) {
                         const float *xa = reinterpret_cast<const float *>(S + size_t(2 * p) * NHP) + off;
                         const float *xb = xa + G::RP;
@@ -80,7 +88,7 @@ B200_HD void row_forward(const Ex &ex, float2 *S, int P, const float2 *TW, int o
                     }
                 },
                 [&](int lane, St &s) {
-                    const int p = 2 * g + (lane & 1), n2 = lane >> 1;
+                    const int p = pair_of(g, lane >> 4), n2 = lane & 15;
                     if (p < P && n2 < N2) {
                         float2 *e = S + size_t(2 * p) * NHP;
 #pragma unroll
@@ -88,14 +96,14 @@ B200_HD void row_forward(const Ex &ex, float2 *S, int P, const float2 *TW, int o
                     }
                 },
                 [&](int lane, St &s) {   // step 2
-                    const int p = 2 * g + (lane & 1), k1 = lane >> 1;
+                    const int p = pair_of(g, lane >> 4), k1 = lane & 15;
                     if (p < P) {
                         const float2 *e = S + size_t(2 * p) * NHP;
                         fwd_step2<N>(k1, s.z, [&](int q) { return e[q]; });
                     }
                 },
                 [&](int lane, St &s) {   // the row transform in natural order
-                    const int p = 2 * g + (lane & 1), k1 = lane >> 1;
+                    const int p = pair_of(g, lane >> 4), k1 = lane & 15;
                     if (p < P) {
                         float2 *e = S + size_t(2 * p) * NHP;
 #pragma unroll
@@ -103,7 +111,7 @@ B200_HD void row_forward(const Ex &ex, float2 *S, int P, const float2 *TW, int o
                     }
                 },
                 [&](int lane, St &s) {   // the two half spectra
-                    const int p = 2 * g + (lane & 1), j = lane >> 1;
+                    const int p = pair_of(g, lane >> 4), j = lane & 15;
                     if (p < P) {
                         const float2 *e = S + size_t(2 * p) * NHP;
 #pragma unroll
@@ -114,7 +122,7 @@ B200_HD void row_forward(const Ex &ex, float2 *S, int P, const float2 *TW, int o
                     }
                 },
                 [&](int lane, St &s) {
-                    const int p = 2 * g + (lane & 1), j = lane >> 1;
+                    const int p = pair_of(g, lane >> 4), j = lane & 15;
                     if (p < P) {
                         float2 *e = S + size_t(2 * p) * NHP;
 #pragma unroll
@@ -225,10 +233,10 @@ B200_HD void row_inverse(const Ex &ex, float2 *S, int M, const float2 *TWI, Norm
     const int P = (M + 1) / 2;
     float *Sr = reinterpret_cast<float *>(S);
     ex.for_warps([&](int warp) {
-        for (int g = warp; 2 * g < P; g += ex.nwarps()) {
+        for (int g = warp; g < pair_items(P); g += ex.nwarps()) {
             ex.template run<St>(
                 [&](int lane, St &s) {   // step 1 on (row u1) + i (row u2), extended to full spectra
-                    const int p = 2 * g + (lane & 1), k1 = lane >> 1;
+                    const int p = pair_of(g, lane >> 4), k1 = lane & 15;
                     const int u1 = 2 * p, u2 = 2 * p + 1;
                     if (p < P) {
                         const float2 *h1 = S + size_t(u1) * NHP, *h2 = S + size_t(u2) * NHP;
@@ -243,7 +251,7 @@ B200_HD void row_inverse(const Ex &ex, float2 *S, int M, const float2 *TWI, Norm
                     }
                 },
                 [&](int lane, St &s) {
-                    const int p = 2 * g + (lane & 1), k1 = lane >> 1;
+                    const int p = pair_of(g, lane >> 4), k1 = lane & 15;
                     if (p < P) {
                         float2 *e = S + size_t(2 * p) * NHP;
 #pragma unroll
@@ -251,14 +259,14 @@ B200_HD void row_inverse(const Ex &ex, float2 *S, int M, const float2 *TWI, Norm
                     }
                 },
                 [&](int lane, St &s) {   // step 2
-                    const int p = 2 * g + (lane & 1), n2 = lane >> 1;
+                    const int p = pair_of(g, lane >> 4), n2 = lane & 15;
                     if (p < P && n2 < N2) {
                         const float2 *e = S + size_t(2 * p) * NHP;
                         inv_step2<N>(n2, s.y, [&](int q) { return e[q]; });
                     }
                 },
                 [&](int lane, St &s) {   // the two rows, normalized, as floats
-                    const int p = 2 * g + (lane & 1), n2 = lane >> 1;
+                    const int p = pair_of(g, lane >> 4), n2 = lane & 15;
                     const int u1 = 2 * p, u2 = 2 * p + 1;
                     if (p < P && n2 < N2) {
 #pragma unroll
