@@ -276,6 +276,29 @@ def test_big_transform_surfaces_match_fp64_oracle():
     assert np.nanmax(d) < 1e-3
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize('window,search', [(127, 64), (130, 60), (200, 10)])
+def test_big_transform_cluster_geometries(window, search):
+    """The two-CTA cluster form of the N = 256 transform at other geometries than the golden case: odd
+    L (the last chip row padded), other surface sizes (other splits of the M rows between the two
+    CTAs), a small search. Surfaces and offsets against the FP64 direct oracle."""
+    from slipcam_b200 import synth
+    h, w = 360, 400
+    frames = synth.video(h, w, 2, np.array([[0.0, 0.0], [1.3, -2.2]]), np.zeros(2), sigma=2.0, noise=1.0, seed=21)
+    down, across = framecor.window_grid(h, w, window, search, 48)
+    down, across = down[:2], across[:2]
+    cor = framecor.Correlator(h, w, down, across, window=window, search=search, backend='b200')
+    cor.set_reference(frames[0])
+    assert cor.info()[2] == 256
+    out = cor.correlate(torch.as_tensor(frames[1:]).cuda(), surfaces=True)
+    o = oracle.correlate(h, w, down, across, frames[0], frames[1:], None, window=window, search=search, mode='f64',
+                         surfaces=True)
+    assert np.abs(out['surface'].cpu().numpy() - o['surface']).max() < 2e-5
+    d = np.abs(out['offsets'].cpu().numpy() - o['offsets64'])
+    assert np.array_equal(np.isnan(d), np.isnan(o['offsets64']))
+    assert np.nanmax(d) < 1e-3
+
+
 def test_search_beyond_big_transform_rejected():
     """Past the staged transform's limit (search 64 at L up to 256) a clear ValueError."""
     down, across = framecor.window_grid(512, 512, 32, 100, 64)   # L = 232, M = 201
