@@ -233,9 +233,11 @@ def _stab_check(rc, ctx):
 
 def warp(frame, params, fill=None):
     """The frame resampled onto the reference (stabilize.py:99-106): the value at (x, y) of the
-    reference is that of the frame at the transformed position (bilinear); outside the frame, fill
-    (default: the frame's mean, numpy's). frame: height x width, a numpy array or a CUDA tensor;
-    returns float32 of the same kind."""
+    reference is that of the frame at the transformed position (bilinear); outside the frame, fill.
+    The default fill is the frame's mean: numpy's for a numpy frame (the reference's value); for a
+    CUDA tensor its float64 mean, which can differ from numpy's float32 mean in the last bits.
+    stabilize() computes numpy's float32 mean on the GPU itself. frame: height x width, a numpy
+    array or a CUDA tensor; returns float32 of the same kind."""
     import torch
     on_device = isinstance(frame, torch.Tensor) and frame.is_cuda
     if fill is None:
