@@ -204,9 +204,13 @@ B200_API int b200_coarse_fit_device(const double *peaks, int32_t *gross, const u
  * positions predicted by the previous one, its transform written to params (n x 4 doubles) and the
  * windows of its fit to used (n int32). keep (windows bytes): the templates in use. gross
  * (windows x 2 int32) and prev (4 doubles) carry the prediction from call to call; reset != 0 zeroes
- * them first (the start of a pass from the reference). Per group of frames the tables in one batch,
- * then per frame three launches: the FP32 correlation (whatever the handle's form), the peaks, the
- * fit. The handle keeps one frame's surfaces and peaks (allocated by the first call). */
+ * them first (the start of a pass from the reference). Per group of frames the tables in one batch
+ * (on a side stream, a group ahead), then per frame two launches: the FP32 correlation with the
+ * peaks (whatever the handle's form) and the fit. The chain runs on the handle's own stream, ordered
+ * after the work already on `stream` and before any work put there later; the reference spectra
+ * stay in L2 there (an access-policy window; the first call raises the context's persisting-L2
+ * limit to their size). The handle keeps one frame's peaks and outputs (allocated by the first
+ * call). */
 B200_API int b200_coarse_track_device(b200_handle *h, const uint8_t *frames, int n, int pitch, const uint8_t *keep,
                                       double min_peak, int reset, int32_t *gross, double *prev, double *params,
                                       int32_t *used, void *stream);

@@ -356,7 +356,8 @@ struct b200_handle {
     DevBuf<CUtensorMap> d_tmaps; // TMA maps of the three denominator tables: slot 0, slot 1, device path
     DevBuf<float> d_coarse;      // coarse tracking: one frame's surfaces and four outputs
     DevBuf<double> d_cpeaks;     // coarse tracking: one frame's peaks
-    cudaEvent_t coarse_ev[5] = {};  // coarse tracking: tables ready (2), tables consumed (2), call start
+    cudaEvent_t coarse_ev[6] = {};  // coarse tracking: tables ready (2), tables consumed (2), call start, end
+    bool coarse_l2 = false;      // the handle's stream keeps the reference spectra in L2
     bool tc_ok = false;          // the geometry fits the tensor-core kernel
     int fpitch = 0;              // the pitch of the staged frames (a multiple of 16)
     bool profiling = false;      // events around the correlation launches
@@ -1124,20 +1125,45 @@ int b200_coarse_track_device(b200_handle *h, const uint8_t *frames, int n, int p
         if (!keep || !gross || !prev || (n && (!frames || !params || !used || pitch < h->width)))
             fail(B200_EINVAL, "null input or output, or a pitch below the width");
         CK(cudaSetDevice(h->device));
-        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        cudaStream_t caller = static_cast<cudaStream_t>(stream);
         const size_t nwin = size_t(h->nwin), MM = size_t(h->M) * h->M;
         if (reset) {
-            CK(cudaMemsetAsync(gross, 0, 2 * nwin * sizeof(int32_t), s));
-            CK(cudaMemsetAsync(prev, 0, 4 * sizeof(double), s));
+            CK(cudaMemsetAsync(gross, 0, 2 * nwin * sizeof(int32_t), caller));
+            CK(cudaMemsetAsync(prev, 0, 4 * sizeof(double), caller));
         }
         if (n == 0) return;
+        if (!h->coarse_ev[0])
+            for (cudaEvent_t &e : h->coarse_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        // the frame chain runs on the handle's own stream, after the caller's work and before the
+        // caller's next: there the grid's reference spectra persist in L2 (every frame reads them;
+        // the next group's tables, written beside the chain, would otherwise evict them)
+        cudaStream_t s = h->comp;
+        if (!h->coarse_l2) {
+            cudaDeviceProp prop{};
+            CK(cudaGetDeviceProperties(&prop, h->device));
+            const size_t want = nwin * size_t(h->N / 2 + 1) * h->N * sizeof(float2);
+            const size_t carve = std::min<size_t>(want, size_t(prop.persistingL2CacheMaxSize));
+            size_t cur = 0;
+            CK(cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize));
+            if (carve > cur) CK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, carve));
+            cudaStreamAttrValue v{};
+            v.accessPolicyWindow.base_ptr = h->d_spec.p;
+            v.accessPolicyWindow.num_bytes = std::min<size_t>(want, size_t(prop.accessPolicyMaxWindowSize));
+            v.accessPolicyWindow.hitRatio = carve >= v.accessPolicyWindow.num_bytes
+                                                ? 1.0f
+                                                : float(double(carve) / double(v.accessPolicyWindow.num_bytes));
+            v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+            v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+            CK(cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &v));
+            h->coarse_l2 = true;
+        }
+        CK(cudaEventRecord(h->coarse_ev[4], caller));
+        CK(cudaStreamWaitEvent(s, h->coarse_ev[4], 0));
         // the big transform has no fused peak: its surfaces go through the peak kernel
         const bool fused = h->N != kBigN;
         const size_t work = nwin * (7 + (fused ? 0 : MM));
         if (h->d_coarse.n < work) h->d_coarse.alloc(work);
         if (h->d_cpeaks.n < 3 * nwin) h->d_cpeaks.alloc(3 * nwin);
-        if (!h->coarse_ev[0])
-            for (cudaEvent_t &e : h->coarse_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         float *o = h->d_coarse.p, *surf = fused ? nullptr : o + 7 * nwin;
         const int64_t fstride = int64_t(pitch) * h->height;
         FitArgs fa{h->d_cpeaks.p, gross, keep, h->d_down.p, h->d_across.p, h->W / 2, h->ny, h->nx, h->height,
@@ -1164,8 +1190,7 @@ int b200_coarse_track_device(b200_handle *h, const uint8_t *frames, int n, int p
             CK(cudaEventRecord(ready[g % 2], side));
             h->launches += 3;
         };
-        CK(cudaEventRecord(start, s));   // the frames and the state are written on `stream` before this call
-        CK(cudaStreamWaitEvent(side, start, 0));
+        CK(cudaStreamWaitEvent(side, start, 0));   // the frames and the state are written on the caller's stream
         tables(0);
         for (int g = 0; g < groups; ++g) {
             if (g + 1 < groups) tables(g + 1);
@@ -1193,6 +1218,8 @@ int b200_coarse_track_device(b200_handle *h, const uint8_t *frames, int n, int p
             }
             CK(cudaEventRecord(consumed[g % 2], s));
         }
+        CK(cudaEventRecord(h->coarse_ev[5], s));   // the caller's stream continues after the chain
+        CK(cudaStreamWaitEvent(caller, h->coarse_ev[5], 0));
     });
 }
 
