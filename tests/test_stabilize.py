@@ -380,3 +380,22 @@ def test_stabilize_720p():
     inner &= ~text
     err = np.abs(o[1:].astype(np.int32) - f[0].astype(np.int32))[:, inner]
     assert np.median(err) <= 1 and np.percentile(err, 99) <= 6
+
+
+@pytest.mark.gpu
+def test_coarse_track_on_a_side_stream():
+    """The library runs the frame chain on its own stream, ordered by events after the caller's work
+    and before the caller's next: the same transforms from a non-default torch stream, with the
+    frames produced on that stream just before the call."""
+    import torch
+    from slipcam_b200 import stabilize
+    f, text = GOLD['a_frames'], GOLD['a_text']
+    kw = dict(window=48, step=40, search=12, start=1)
+    a = stabilize.coarse_track(f, 4, text, **kw)
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        fd = torch.as_tensor(f).cuda(non_blocking=False) + 0   # produced on the side stream
+        tr = stabilize.CoarseTracker(fd[4], text, window=48, step=40, search=12)
+        b = tr.run(fd, 4, start=1)
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
