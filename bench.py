@@ -644,6 +644,103 @@ def run_stabilize(args):
     }))
 
 
+def run_scans(args):
+    """
+    auto_slip's scans around the path on the b200 backend (one GPU): frame_differences over a 720p
+    video (300 frames), the burned-in text mask from 150 of its frames (chunks of 10), and
+    periodicity of the reference frame's 720p grid (window 64, search 48, skip 16: 2450 windows).
+    The frame-difference kernel is timed by CUDA events through the C ABI on device-resident frames
+    (its roofline: HBM, two frames read per pair); the rest through the public calls. CPU: the
+    oracle's restatements of the reference functions on bounded samples, one thread.
+    """
+    import ctypes
+
+    import torch
+    from oracle import oracle
+    from slipcam_b200 import _lib, framecor, scans, synth
+    n, h, w = (args.video if args.video != NFRAMES else 300), 720, 1280
+    boxes = ((900, 24, 1240, 68), (40, 650, 630, 700))
+    frames, _, _ = synth.camera(n, h, w, ref=0, seed=15, walk=(1.0, 1.0, 0.0005, 0.0005), text=boxes, device='cuda')
+    host = frames.cpu().numpy()
+    lib, stream = _lib.lib(), torch.cuda.current_stream().cuda_stream
+    out = torch.empty(n - 1, dtype=torch.float32, device='cuda')
+    sums = torch.empty(n - 1, dtype=torch.int64, device='cuda')
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def diff_launch():
+        rc = lib.b200_frame_diff_device(frames.data_ptr(), n, h, w, w, out.data_ptr(), sums.data_ptr(), stream)
+        assert rc == _lib.OK
+    for _ in range(args.warmup):
+        diff_launch()
+    torch.cuda.synchronize()
+    steps = max(1, min(args.steps, 20))
+    e0.record()
+    for _ in range(steps):
+        diff_launch()
+    e1.record()
+    torch.cuda.synchronize()
+    diff_ms = e0.elapsed_time(e1) / steps
+    diff_bytes = float(n) * h * w   # the algorithmic minimum: every frame read once
+    pk = peaks()
+    hbm = pk.get('hbm_gbs', 6650.0)
+    d_gpu = scans.frame_differences(host)   # from host memory, the public call
+    t = time.perf_counter()
+    scans.frame_differences(host)
+    diff_e2e_s = time.perf_counter() - t
+    cpu_n = 60
+    t = time.perf_counter()
+    d_cpu = oracle.frame_differences(host[:cpu_n])
+    diff_cpu_s = time.perf_counter() - t
+
+    def timed(call, reps=3):
+        call()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            t = time.perf_counter()
+            r = call()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t)
+        return statistics.median(ts), r
+    tm_s, mask = timed(lambda: scans.text_mask(frames, 0, nframes=150, chunk=10))
+    tm_e2e_s, mask_h = timed(lambda: scans.text_mask(host, 0, nframes=150, chunk=10))
+    t = time.perf_counter()
+    mask_cpu = oracle.text_mask(host, 0, nframes=150, chunk=10)
+    tm_cpu_s = time.perf_counter() - t
+    down, across = framecor.window_grid(h, w, 64, 48, 16)
+    per_s, per = timed(lambda: framecor.periodicity(frames[0], down, across, 64, 48))
+    sub_d, sub_a = down[::9][:3], across[::14][:5]
+    t = time.perf_counter()
+    per_cpu = oracle.periodicity(host[0], sub_d, sub_a, 64, 48)
+    per_cpu_s = time.perf_counter() - t
+    print(json.dumps({
+        'metric': 'frames/s, auto_slip frame differences of a 720p video', 'value': (n - 1) / (diff_ms / 1e3),
+        'unit': 'frames/s', 'n_gpus': 1, 'steps': steps, 'warmup': args.warmup, 'ms_per_step': diff_ms,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'u8 -> int64 sums',
+        'data': 'synthetic',
+        'config': {'workload': f'720p camera video, {n} frames, two burned-in text boxes; text mask from 150 frames '
+                               '(chunks of 10); periodicity of the reference frame, window 64, search 48, skip 16 '
+                               f'({len(down) * len(across)} windows)', 'l2': f'{n} frames = {n * h * w / 1e6:.0f} MB > L2'},
+        'roofline': {'bound': 'hbm', 'achieved': diff_bytes / (diff_ms / 1e3) / 1e9, 'peak': hbm, 'unit': 'GB/s',
+                     'frac': diff_bytes / (diff_ms / 1e3) / 1e9 / hbm, 'kernel': 'frame_diff_kernel',
+                     'algorithmic_bytes': 'every frame read once (n x 720 x 1280 bytes)', 'traffic': None,
+                     'peak_source': 'MEASURED_PEAKS.json hbm_gbs' if 'hbm_gbs' in pk else 'fallback 6.65 TB/s'},
+        'e2e': {'value': (n - 1) / diff_e2e_s, 'unit': 'frames/s', 'h2d_bytes_per_step': n * h * w,
+                'd2h_bytes_per_step': (n - 1) * 4, 'path': 'scans.frame_differences over a host array'},
+        'gpu_launches': 1,
+        'cpu_baseline': {'value': (cpu_n - 1) / diff_cpu_s, 'unit': 'frames/s', 'cores': 1, 'kind': 'port',
+                         'sample': f'{cpu_n} frames ({diff_cpu_s:.2f} s)'},
+        'agreement': {'frame_differences_equal': bool(np.array_equal(d_gpu[:cpu_n - 1], d_cpu)),
+                      'text_mask_equal': bool(np.array_equal(mask, mask_cpu) and np.array_equal(mask_h, mask_cpu)),
+                      'periodicity_max_abs': float(np.abs(per[::9][:3, ::14][:, :5] - per_cpu).max())},
+        'text_mask': {'ms': tm_s * 1e3, 'ms_from_host': tm_e2e_s * 1e3, 'cpu_ms': tm_cpu_s * 1e3,
+                      'cpu_kind': 'port, 1 thread', 'pixels': int(mask.sum())},
+        'periodicity': {'windows_per_s': len(down) * len(across) / per_s, 'ms': per_s * 1e3,
+                        'cpu_windows_per_s': per_cpu.size / per_cpu_s,
+                        'cpu_sample': f'{per_cpu.size} windows, FP64 direct restatement ({per_cpu_s:.1f} s)'},
+    }))
+
+
 def main():
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     p.add_argument('--gpus', type=int, default=1)
@@ -656,9 +753,10 @@ def main():
     p.add_argument('--video', type=int, default=NFRAMES, help='frames of the synthetic video to render')
     p.add_argument('--batch', type=int, default=BATCH, help='frames per step')
     p.add_argument('--form', default='tc', choices=['fft32', 'tc'], help='the arithmetic of the transforms')
-    p.add_argument('--workload', default='hd', choices=['hd', 'mixed', 'stream', 'diff', 'stabilize'],
+    p.add_argument('--workload', default='hd', choices=['hd', 'mixed', 'stream', 'diff', 'stabilize', 'scans'],
                    help='hd: the 720p headline; mixed: three grids in one group step; stream: 1080p streaming; '
-                        'diff: the differentiable path; stabilize: coarse similarity tracking')
+                        'diff: the differentiable path; stabilize: coarse similarity tracking; '
+                        'scans: frame differences, text mask, periodicity')
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.workload == 'mixed' and args.impl != 'reference':
@@ -669,6 +767,8 @@ def main():
         run_diff(args)
     elif args.workload == 'stabilize' and args.impl != 'reference':
         run_stabilize(args)
+    elif args.workload == 'scans' and args.impl != 'reference':
+        run_scans(args)
     elif args.impl == 'reference':
         run_reference(args)
     else:

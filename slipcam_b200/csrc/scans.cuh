@@ -15,32 +15,84 @@ constexpr int kScanMaxChunks = 64;   // chunks of the temporal median (nframes /
 
 #ifdef __CUDACC__
 
-// sum |f[k + 1] - f[k]| over the pixels, exact (64-bit), one CTA per (pair, band of rows)
+constexpr int kDiffRun = 16;   // consecutive pairs of frames per CTA of the difference scan
+
+// sum |f[k + 1] - f[k]| over the pixels, exact (64-bit), for the pairs k0 .. k0 + kDiffRun - 1 of
+// this CTA's run (blockIdx.y) over its band of rows (blockIdx.x): each thread walks a word (4
+// pixels) or a pixel through the run's frames with the previous frame's value in a register, so
+// every frame of the run is read once; the run's loads are independent, issued back to back
 __global__ void __launch_bounds__(256) frame_diff_kernel(const uint8_t *__restrict__ frames, int64_t fstride, int pitch,
-                                                           int h, int w, unsigned long long *__restrict__ sums)
+                                                           int h, int w, int npairs, unsigned long long *__restrict__ sums)
 {
-    const int k = blockIdx.y;
-    const uint8_t *a = frames + k * fstride, *b = a + fstride;
-    unsigned long long s = 0;
+    const int k0 = blockIdx.y * kDiffRun, K = min(kDiffRun, npairs - k0);
     const int rows = (h + gridDim.x - 1) / gridDim.x, r0 = blockIdx.x * rows, r1 = min(h, r0 + rows);
-    for (int r = r0; r < r1; ++r) {
-        const uint8_t *pa = a + int64_t(r) * pitch, *pb = b + int64_t(r) * pitch;
-        if (((pitch | reinterpret_cast<uintptr_t>(a)) & 3) == 0) {
-            const int wq = w / 4;
-            for (int c = threadIdx.x; c < wq; c += blockDim.x) {
-                const uint32_t x = reinterpret_cast<const uint32_t *>(pa)[c], y = reinterpret_cast<const uint32_t *>(pb)[c];
-                s += __vabsdiffu4(x, y) & 0xFFu;
-                s += (__vabsdiffu4(x, y) >> 8) & 0xFFu;
-                s += (__vabsdiffu4(x, y) >> 16) & 0xFFu;
-                s += __vabsdiffu4(x, y) >> 24;
+    unsigned long long acc[kDiffRun];
+#pragma unroll
+    for (int j = 0; j < kDiffRun; ++j) acc[j] = 0;
+    if (r0 < r1) {
+        const uint8_t *f0 = frames + k0 * fstride;
+        const int align = pitch | int(fstride & 15) | int(reinterpret_cast<uintptr_t>(frames) & 15);
+        // 16 pixels per load where rows and frames are 16-byte aligned: enough bytes in flight
+        const int w16 = (align & 15) == 0 ? w / 16 : 0;
+        if (w16 > 0) {
+            const int64_t fv = fstride / 16, n_el = int64_t(r1 - r0) * w16;
+            for (int64_t e = threadIdx.x; e < n_el; e += blockDim.x) {
+                const int r = r0 + int(e / w16), c = int(e % w16);
+                const uint4 *p = reinterpret_cast<const uint4 *>(f0 + int64_t(r) * pitch) + c;
+                uint4 prev = __ldg(p);
+#pragma unroll
+                for (int j = 0; j < kDiffRun; ++j) {
+                    if (j < K) {
+                        const uint4 cur = __ldg(p + (j + 1) * fv);
+                        acc[j] += unsigned(__vsadu4(prev.x, cur.x)) + unsigned(__vsadu4(prev.y, cur.y)) +
+                                  unsigned(__vsadu4(prev.z, cur.z)) + unsigned(__vsadu4(prev.w, cur.w));
+                        prev = cur;
+                    }
+                }
             }
-            for (int c = 4 * wq + threadIdx.x; c < w; c += blockDim.x) s += abs(int(pa[c]) - int(pb[c]));
-        } else {
-            for (int c = threadIdx.x; c < w; c += blockDim.x) s += abs(int(pa[c]) - int(pb[c]));
+        }
+        const bool words = (align & 3) == 0;
+        const int wq = words ? (w - 16 * w16) / 4 : 0, cw = 16 * w16;   // words past the 16-pixel pieces
+        if (wq > 0) {
+            const int64_t fw = fstride / 4, n_el = int64_t(r1 - r0) * wq;
+            for (int64_t e = threadIdx.x; e < n_el; e += blockDim.x) {
+                const int r = r0 + int(e / wq), c = int(e % wq);
+                const uint32_t *p = reinterpret_cast<const uint32_t *>(f0 + int64_t(r) * pitch + cw) + c;
+                uint32_t prev = __ldg(p);
+#pragma unroll
+                for (int j = 0; j < kDiffRun; ++j) {
+                    if (j < K) {
+                        const uint32_t cur = __ldg(p + (j + 1) * fw);
+                        const uint32_t d = __vabsdiffu4(prev, cur);
+                        acc[j] += (d & 0xFFu) + ((d >> 8) & 0xFFu) + ((d >> 16) & 0xFFu) + (d >> 24);
+                        prev = cur;
+                    }
+                }
+            }
+        }
+        // the columns past the words (or every column when the frames are not word-aligned)
+        const int c0 = cw + 4 * wq, tail = w - c0;
+        const int64_t n_tail = int64_t(r1 - r0) * tail;
+        for (int64_t e = threadIdx.x; e < n_tail; e += blockDim.x) {
+            const int r = r0 + int(e / tail), c = c0 + int(e % tail);
+            const uint8_t *p = f0 + int64_t(r) * pitch + c;
+            int prev = p[0];
+#pragma unroll
+            for (int j = 0; j < kDiffRun; ++j) {
+                if (j < K) {
+                    const int cur = p[(j + 1) * fstride];
+                    acc[j] += unsigned(abs(cur - prev));
+                    prev = cur;
+                }
+            }
         }
     }
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(sums + k, s);
+#pragma unroll
+    for (int j = 0; j < kDiffRun; ++j) {
+        unsigned long long v = acc[j];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0 && j < K && v) atomicAdd(sums + k0 + j, v);
+    }
 }
 
 // per pixel: the population standard deviation of each chunk of `chunk` frames (exact integer

@@ -53,3 +53,26 @@ def test_b200_text_mask_fills_a_large_box():
     m = scans.text_mask(f, 0, nframes=20, chunk=10, dilate=1)
     assert m[150, 200] and m[22, 22] and not m[5, 5]
     assert np.array_equal(m, oracle.text_mask(f, 0, nframes=20, chunk=10, dilate=1))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('width,offset', [(167, 1), (168, 2), (150, 0), (33, 3)])
+def test_frame_differences_any_alignment(width, offset):
+    """The difference scan's 16-pixel, word and byte paths: frames at a base address `offset` bytes
+    past an aligned one and of any width, through the C ABI, against the oracle."""
+    import ctypes
+
+    import torch
+    from slipcam_b200 import _lib
+    f = np.ascontiguousarray(golden()['frames'][:21, :, :width])
+    n, h, w = f.shape
+    buf = torch.zeros(n * h * w + 16, dtype=torch.uint8, device='cuda')
+    buf[offset:offset + n * h * w] = torch.as_tensor(f.ravel()).cuda()
+    out = torch.empty(n - 1, dtype=torch.float32, device='cuda')
+    sums = torch.empty(n - 1, dtype=torch.int64, device='cuda')
+    rc = _lib.lib().b200_frame_diff_device(buf.data_ptr() + offset, n, h, w, w, out.data_ptr(), sums.data_ptr(),
+                                          torch.cuda.current_stream().cuda_stream)
+    assert rc == _lib.OK
+    exact = np.array([np.abs(f[k + 1].astype(np.int64) - f[k].astype(np.int64)).sum() for k in range(n - 1)])
+    assert np.array_equal(sums.cpu().numpy(), exact)
+    np.testing.assert_array_equal(out.cpu().numpy(), oracle.frame_differences(f))
