@@ -1059,12 +1059,16 @@ int b200_frame_diff_device(const uint8_t *frames, int n, int height, int width, 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     unsigned long long *us = reinterpret_cast<unsigned long long *>(sums);
     if (cudaMemsetAsync(us, 0, size_t(n - 1) * sizeof(uint64_t), s) != cudaSuccess) return B200_ERUNTIME;
-    // runs of kDiffRun pairs, and bands of rows enough for about eight CTAs per SM
-    int dev = 0, sms = 148;
+    // runs of kDiffRun pairs, and bands of rows for two full waves of the CTAs the SMs hold at once
+    int dev = 0, sms = 148, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return B200_ERUNTIME;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, frame_diff_kernel, 256, 0) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 2;
+    }
     const int runs = (n - 1 + kDiffRun - 1) / kDiffRun;
-    const unsigned bands = unsigned(std::clamp((8 * sms + runs - 1) / runs, 1, height));
+    const unsigned bands = unsigned(std::clamp(2 * sms * per_sm / runs, 1, height));
     frame_diff_kernel<<<dim3(bands, unsigned(runs)), 256, 0, s>>>(frames, int64_t(pitch) * height, pitch, height, width,
                                                                   n - 1, us);
     frame_diff_means_kernel<<<blocks_for(n - 1), 256, 0, s>>>(us, n - 1, double(height) * width, out);

@@ -26,7 +26,9 @@ __global__ void __launch_bounds__(256) frame_diff_kernel(const uint8_t *__restri
 {
     const int k0 = blockIdx.y * kDiffRun, K = min(kDiffRun, npairs - k0);
     const int rows = (h + gridDim.x - 1) / gridDim.x, r0 = blockIdx.x * rows, r1 = min(h, r0 + rows);
-    unsigned long long acc[kDiffRun];
+    // a thread's own sums fit 32 bits: at most (its pieces) x 16 x 255, under 2^26 for any frame a
+    // band of rows of an 8K video gives one thread; the warp and the total are 64-bit
+    uint32_t acc[kDiffRun];
 #pragma unroll
     for (int j = 0; j < kDiffRun; ++j) acc[j] = 0;
     if (r0 < r1) {
@@ -44,8 +46,8 @@ __global__ void __launch_bounds__(256) frame_diff_kernel(const uint8_t *__restri
                 for (int j = 0; j < kDiffRun; ++j) {
                     if (j < K) {
                         const uint4 cur = __ldg(p + (j + 1) * fv);
-                        acc[j] += unsigned(__vsadu4(prev.x, cur.x)) + unsigned(__vsadu4(prev.y, cur.y)) +
-                                  unsigned(__vsadu4(prev.z, cur.z)) + unsigned(__vsadu4(prev.w, cur.w));
+                        acc[j] += __vsadu4(prev.x, cur.x) + __vsadu4(prev.y, cur.y) + __vsadu4(prev.z, cur.z) +
+                                  __vsadu4(prev.w, cur.w);
                         prev = cur;
                     }
                 }
@@ -90,7 +92,7 @@ __global__ void __launch_bounds__(256) frame_diff_kernel(const uint8_t *__restri
 #pragma unroll
     for (int j = 0; j < kDiffRun; ++j) {
         unsigned long long v = acc[j];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);   // 64-bit from here
         if ((threadIdx.x & 31) == 0 && j < K && v) atomicAdd(sums + k0 + j, v);
     }
 }
