@@ -256,12 +256,22 @@ B200_API int b200_chunk_std_median_device(const uint8_t *frames, int nchunks, in
 /* out (height x width float32): hypot of the two Sobel derivatives of a frame, borders reflected
  * (scipy.ndimage.sobel, auto_slip.py:91). */
 B200_API int b200_sobel_device(const uint8_t *frame, int height, int width, int pitch, float *out, void *stream);
-/* The text mask from the edge magnitude and the temporal deviation (auto_slip.py:92-94): edge > thr
- * and sd < max_std, `dilate` steps of the 3 x 3 cross dilation, then the holes (background not
- * 4-connected to the border) filled. mask: height x width bytes (0 / 1); scratch: 2 x height x
- * width bytes; flag: one int. Synchronous on `stream` (the fill runs until nothing changes). */
-B200_API int b200_text_mask_device(const float *edge, const float *sd, int height, int width, float thr, float max_std,
-                                   int dilate, uint8_t *mask, uint8_t *scratch, int *flag, void *stream);
+/* *out (device float32) = numpy.percentile(x[0 .. n), q) of n float32 values in device memory,
+ * method 'linear', computed as numpy does for float32 data (the virtual index (n - 1) * (q / 100),
+ * its weight and the interpolation in float32); used for the text mask's edge threshold
+ * (auto_slip.py:92). q in [0, 100], 1 <= n < 2^32; scratch: B200_PERCENTILE_SCRATCH bytes of
+ * device memory. Stream-ordered, no host synchronisation. */
+#define B200_PERCENTILE_SCRATCH 16640
+B200_API int b200_percentile_f32_device(const float *x, int64_t n, double q, float *out, void *scratch, void *stream);
+/* The text mask from the edge magnitude and the temporal deviation (auto_slip.py:92-94): edge above
+ * numpy.percentile(edge, edge_percentile) and sd < max_std, `dilate` steps of the 3 x 3 cross
+ * dilation, then the holes (background not 4-connected to the border) filled. mask: height x width
+ * bytes (0 / 1); scratch: b200_text_mask_scratch_bytes(height, width) bytes of device memory.
+ * Stream-ordered, no host synchronisation. Widths up to 28,000 pixels. */
+B200_API size_t b200_text_mask_scratch_bytes(int height, int width);
+B200_API int b200_text_mask_device(const float *edge, const float *sd, int height, int width, double edge_percentile,
+                                   float max_std, int dilate, uint8_t *mask, void *scratch, size_t scratch_bytes,
+                                   void *stream);
 
 /* ---- The differentiable path: float frames, a continuous shift per pair, and the adjoints.
  * No counterpart in the reference (its backends take uint8 frames and give no derivatives); the

@@ -241,7 +241,18 @@ def text_mask(frames, start, nframes=150, chunk=10, edge_percentile=90, max_std=
     max_std) pixels, dilated `dilate` times by the 3 x 3 cross, then every background region that
     does not touch the border (4-connected) filled.
     """
-    from scipy import ndimage
+    f = np.asarray(frames)
+    sd = chunk_std_median(f, start, nframes, chunk)
+    edge = _sobel_magnitude(f[start].astype(np.float32))
+    return mask_from_maps(edge, sd, edge_percentile, max_std, dilate)
+
+
+def chunk_std_median(frames, start, nframes=150, chunk=10):
+    """
+    TEST INFRASTRUCTURE. The steadiness map of auto_slip.text_mask (auto_slip.py:87-90): per pixel,
+    the population standard deviation of each chunk of `chunk` frames from `start` (exact integer
+    sums, float32 result), then the median over the chunks (float32).
+    """
     f = np.asarray(frames)
     stds = []
     for a in range(start, min(start + nframes, len(f)) - chunk + 1, chunk):
@@ -249,8 +260,17 @@ def text_mask(frames, start, nframes=150, chunk=10, edge_percentile=90, max_std=
         s1, s2 = x.sum(0), (x * x).sum(0)
         var = (chunk * s2 - s1 * s1) / float(chunk * chunk)
         stds.append(np.sqrt(np.maximum(var, 0)).astype(np.float32))
-    sd = np.median(np.stack(stds), axis=0)
-    edge = _sobel_magnitude(f[start].astype(np.float32))
+    return np.median(np.stack(stds), axis=0)
+
+
+def mask_from_maps(edge, sd, edge_percentile=90, max_std=1.5, dilate=4):
+    """
+    TEST INFRASTRUCTURE. The rest of auto_slip.text_mask (auto_slip.py:92-94) from the float32 edge
+    magnitude and steadiness maps: pixels above numpy.percentile(edge, edge_percentile) and below
+    max_std, dilated `dilate` times by the 3 x 3 cross, then every background region that does not
+    touch the border (4-connected) filled.
+    """
+    from scipy import ndimage
     m = (edge > np.percentile(edge, edge_percentile)) & (sd < max_std)
     for _ in range(dilate):
         g = m.copy()

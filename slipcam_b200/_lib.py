@@ -13,6 +13,7 @@ OK, EINVAL, ERUNTIME, ETIMEOUT = 0, 1, 2, 3
 GROSS_NONE, GROSS_FRAME, GROSS_WINDOW = 0, 1, 2
 FORM_AUTO, FORM_FFT32, FORM_TC = 0, 1, 2
 COARSE_MAX_WINDOWS = 2048
+PERCENTILE_SCRATCH = 16640   # bytes of device scratch of b200_percentile_f32_device
 
 
 class Params(ctypes.Structure):
@@ -59,7 +60,10 @@ SIGNATURES = {
     'b200_frame_diff_device': (_i, [_vp, _i, _i, _i, _i, _vp, _vp, _vp]),
     'b200_chunk_std_median_device': (_i, [_vp, _i, _i, _i, _i, _i, _vp, _vp]),
     'b200_sobel_device': (_i, [_vp, _i, _i, _i, _vp, _vp]),
-    'b200_text_mask_device': (_i, [_vp, _vp, _i, _i, ctypes.c_float, ctypes.c_float, _i, _vp, _vp, _vp, _vp]),
+    'b200_percentile_f32_device': (_i, [_vp, ctypes.c_int64, ctypes.c_double, _vp, _vp, _vp]),
+    'b200_text_mask_scratch_bytes': (ctypes.c_size_t, [_i, _i]),
+    'b200_text_mask_device': (_i, [_vp, _vp, _i, _i, ctypes.c_double, ctypes.c_float, _i, _vp, _vp, ctypes.c_size_t,
+                                   _vp]),
     'b200_set_reference_f32_device': (_i, [_vp, _vp, _i, _vp]),
     'b200_diff_forward': (_i, [_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     'b200_diff_backward': (_i, [_vp, _vp, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -1078,10 +1078,24 @@ int b200_frame_diff_device(const uint8_t *frames, int n, int height, int width, 
 int b200_chunk_std_median_device(const uint8_t *frames, int nchunks, int chunk, int height, int width, int pitch,
                                  float *out, void *stream)
 {
-    if (nchunks < 1 || nchunks > kScanMaxChunks || chunk < 1 || height <= 0 || width <= 0 || pitch < width || !frames || !out)
+    if (nchunks < 1 || nchunks > kScanMaxChunks || chunk < 1 || chunk > 65536 || height <= 0 || width <= 0 || pitch < width ||
+        !frames || !out)
         return B200_EINVAL;
-    chunk_std_median_kernel<<<blocks_for(int64_t(height) * width), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        frames, int64_t(pitch) * height, pitch, height, width, chunk, nchunks, out);
+    // a frame with contiguous rows is one long row: whole CTAs of pixels and 16-byte loads throughout
+    const int64_t fstride = int64_t(pitch) * height;
+    int rows = height, cols = width, step = pitch;
+    if (pitch == width && int64_t(height) * width <= INT32_MAX) {
+        cols = height * width;
+        rows = 1;
+        step = cols;
+    }
+    const size_t smem = size_t(nchunks) * kStdPixels * sizeof(float);
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(chunk_std_median_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+        return B200_ERUNTIME;
+    const dim3 block(32, unsigned(std::min(nchunks, kStdRegChunks)));
+    chunk_std_median_kernel<<<dim3(unsigned((cols + kStdPixels - 1) / kStdPixels), unsigned(rows)), block, smem,
+                              static_cast<cudaStream_t>(stream)>>>(frames, fstride, step, rows, cols, chunk, nchunks, out);
     return cudaGetLastError() == cudaSuccess ? B200_OK : B200_ERUNTIME;
 }
 
@@ -1093,33 +1107,83 @@ int b200_sobel_device(const uint8_t *frame, int height, int width, int pitch, fl
     return cudaGetLastError() == cudaSuccess ? B200_OK : B200_ERUNTIME;
 }
 
-int b200_text_mask_device(const float *edge, const float *sd, int height, int width, float thr, float max_std, int dilate,
-                          uint8_t *mask, uint8_t *scratch, int *flag, void *stream)
+namespace {
+
+// the three selection passes of numpy.percentile(x[0 .. n), q) into *out (device), q in [0, 100]:
+// the virtual index, its floor and the weight in float32, as numpy computes them for float32 data
+int launch_percentile(const float *x, int64_t n, double q, float *out, void *scratch, cudaStream_t s)
 {
-    if (height <= 0 || width <= 0 || dilate < 0 || !edge || !sd || !mask || !scratch || !flag) return B200_EINVAL;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!x || !out || !scratch || n < 1 || n > int64_t(UINT32_MAX) || !(q >= 0.0 && q <= 100.0)) return B200_EINVAL;
+    const float vi = float(n - 1) * (float(q) / 100.0f);
+    uint32_t lo = uint32_t(n - 1), hi = lo;
+    float t = 1.0f;   // past the last index: both statistics are the largest value
+    if (vi < float(n - 1)) {
+        lo = uint32_t(std::floor(vi));
+        hi = lo + 1;
+        t = vi - float(lo);
+    }
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return B200_ERUNTIME;
+    auto *st = static_cast<SelectState *>(scratch);
+    auto *hist = reinterpret_cast<uint32_t *>(static_cast<char *>(scratch) + 256);
+    if (cudaMemsetAsync(scratch, 0, kSelectScratch, s) != cudaSuccess) return B200_ERUNTIME;
+    const unsigned grid = unsigned(std::clamp<int64_t>((n + 1023) / 1024, 1, 2 * sms));
+    for (int pass = 0; pass < 3; ++pass) select_pass_kernel<<<grid, 256, 0, s>>>(x, n, pass, lo, hi, t, st, hist, out);
+    return cudaGetLastError() == cudaSuccess ? B200_OK : B200_ERUNTIME;
+}
+
+}   // namespace
+
+int b200_percentile_f32_device(const float *x, int64_t n, double q, float *out, void *scratch, void *stream)
+{
+    return launch_percentile(x, n, q, out, scratch, static_cast<cudaStream_t>(stream));
+}
+
+size_t b200_text_mask_scratch_bytes(int height, int width)
+{
+    if (height <= 0 || width <= 0) return 0;
+    return size_t(kSelectScratch) + 2 * size_t(height) * size_t((width + 31) / 32) * 4;
+}
+
+int b200_text_mask_device(const float *edge, const float *sd, int height, int width, double edge_percentile, float max_std,
+                          int dilate, uint8_t *mask, void *scratch, size_t scratch_bytes, void *stream)
+{
+    if (height <= 0 || width <= 0 || dilate < 0 || !edge || !sd || !mask || !scratch) return B200_EINVAL;
     const int64_t n = int64_t(height) * width;
-    const unsigned nb = blocks_for(n);
-    uint8_t *a = scratch, *b = scratch + n;
-    text_seed_kernel<<<nb, 256, 0, s>>>(edge, sd, n, thr, max_std, a);
-    for (int i = 0; i < dilate; ++i) {
-        dilate_kernel<<<nb, 256, 0, s>>>(a, b, height, width);
-        std::swap(a, b);
-    }
-    // the background reached from the border; a step spreads it one pixel, so check every 32
-    outside_init_kernel<<<nb, 256, 0, s>>>(a, b, height, width);
-    for (int64_t done = 0; done < n; done += 32) {
-        if (cudaMemsetAsync(flag, 0, sizeof(int), s) != cudaSuccess) return B200_ERUNTIME;
-        for (int i = 0; i < 32; ++i) outside_step_kernel<<<nb, 256, 0, s>>>(a, b, height, width, flag);
-        int changed = 0;
-        if (cudaMemcpyAsync(&changed, flag, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-            cudaStreamSynchronize(s) != cudaSuccess)
+    const int wpr = (width + 31) / 32;
+    const size_t tile = size_t(2) * (kDilateRows + 2 * kDilateStep) * wpr * 4;   // the dilation's shared memory
+    if (scratch_bytes < b200_text_mask_scratch_bytes(height, width) || n > int64_t(INT32_MAX) || tile > 227 * 1024)
+        return B200_EINVAL;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    float *thr = reinterpret_cast<float *>(static_cast<char *>(scratch) + sizeof(SelectState));
+    if (int rc = launch_percentile(edge, n, edge_percentile, thr, scratch, s); rc != B200_OK) return rc;
+    uint32_t *m = reinterpret_cast<uint32_t *>(static_cast<char *>(scratch) + kSelectScratch), *o = m + int64_t(height) * wpr;
+    text_seed_bits_kernel<<<unsigned((int64_t(height) * wpr * 32 + 255) / 256), 256, 0, s>>>(edge, sd, height, width, wpr,
+                                                                                             thr, max_std, m);
+    for (int done = 0; done < dilate; done += kDilateStep) {
+        const int steps = std::min(kDilateStep, dilate - done);
+        const size_t bytes = size_t(2) * (kDilateRows + 2 * steps) * wpr * 4;
+        if (bytes > 48 * 1024 &&
+            cudaFuncSetAttribute(dilate_bits_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)) != cudaSuccess)
             return B200_ERUNTIME;
-        if (!changed) break;
+        dilate_bits_kernel<<<unsigned((height + kDilateRows - 1) / kDilateRows), 256, bytes, s>>>(m, o, height, width, wpr,
+                                                                                                 steps);
+        std::swap(m, o);
     }
-    fill_kernel<<<nb, 256, 0, s>>>(b, mask, n);
-    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return B200_ERUNTIME;
-    return B200_OK;
+    // the hole filling's two planes in shared memory when they fit (720p: 225 KB)
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+        return B200_ERUNTIME;
+    const size_t planes = size_t(2) * height * wpr * 4;
+    const bool in_smem = planes <= size_t(optin);
+    if (in_smem && planes > 48 * 1024 &&
+        cudaFuncSetAttribute(flood_bits_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(planes)) != cudaSuccess)
+        return B200_ERUNTIME;
+    flood_bits_kernel<<<1, kFloodThreads, in_smem ? planes : 0, s>>>(m, o, height, width, wpr, in_smem ? 1 : 0);
+    fill_bits_kernel<<<blocks_for(n), 256, 0, s>>>(o, height, width, wpr, mask);
+    return cudaGetLastError() == cudaSuccess ? B200_OK : B200_ERUNTIME;
 }
 
 int b200_coarse_track_device(b200_handle *h, const uint8_t *frames, int n, int pitch, const uint8_t *keep,

@@ -12,6 +12,11 @@
 namespace b200 {
 
 constexpr int kScanMaxChunks = 64;   // chunks of the temporal median (nframes / chunk)
+constexpr int kSelectBins = 2048;     // bins of a pass of the percentile's radix selection (11 bits)
+constexpr int kSelectScratch = 256 + 2 * kSelectBins * 4;   // its state and two histograms, bytes
+constexpr int kDilateRows = 16;       // rows a CTA of the bit dilation writes
+constexpr int kDilateStep = 8;        // dilation steps per launch (the tile's halo rows)
+constexpr int kFloodThreads = 1024;   // the one CTA of the hole filling
 
 #ifdef __CUDACC__
 
@@ -99,31 +104,91 @@ __global__ void __launch_bounds__(256) frame_diff_kernel(const uint8_t *__restri
 
 // per pixel: the population standard deviation of each chunk of `chunk` frames (exact integer
 // sums, the root in float), then their median over nchunks (the mean of the two middle values
-// when nchunks is even, as numpy.median)
-__global__ void __launch_bounds__(256) chunk_std_median_kernel(const uint8_t *__restrict__ frames, int64_t fstride, int pitch,
-                                                                 int h, int w, int chunk, int nchunks, float *__restrict__ out)
+// when nchunks is even, as numpy.median). A CTA takes kStdPixels pixels of a row (a frame whose
+// rows are contiguous comes as one long row), 16 per lane in one 16-byte load where aligned;
+// warp y sums chunks y, y + blockDim.y, ... so the loads of every chunk are in flight together.
+// The deviations meet in shared memory (chunk m's slot t holds the lane's pixel t / 32 of lane
+// t % 32) and thread t sorts slot t's column: in registers by odd-even transposition up to
+// kStdRegChunks chunks, in place in shared memory above.
+constexpr int kStdLanePixels = 16;
+constexpr int kStdPixels = 32 * kStdLanePixels;
+constexpr int kStdRegChunks = 16;
+
+__global__ void __launch_bounds__(512, 2) chunk_std_median_kernel(const uint8_t *__restrict__ frames, int64_t fstride, int pitch,
+                                                                    int h, int w, int chunk, int nchunks, float *__restrict__ out)
 {
-    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= int64_t(h) * w) return;
-    const int r = int(i / w), c = int(i % w);
-    float v[kScanMaxChunks];
-    for (int m = 0; m < nchunks; ++m) {
-        int s1 = 0, s2 = 0;
-        for (int t = 0; t < chunk; ++t) {
-            const int x = frames[(int64_t(m) * chunk + t) * fstride + int64_t(r) * pitch + c];
-            s1 += x;
-            s2 += x * x;
+    extern __shared__ float v[];   // [nchunks][kStdPixels]
+    const int r = blockIdx.y, c0 = blockIdx.x * kStdPixels, lane = threadIdx.x;
+    const int c = c0 + kStdLanePixels * lane;
+    const uint8_t *row = frames + int64_t(r) * pitch + c;
+    const bool vec = ((reinterpret_cast<uintptr_t>(row) | uintptr_t(fstride)) & 15) == 0 && c + kStdLanePixels <= w;
+    for (int m = threadIdx.y; m < nchunks; m += blockDim.y) {
+        uint32_t s1[kStdLanePixels], s2[kStdLanePixels];
+#pragma unroll
+        for (int j = 0; j < kStdLanePixels; ++j) s1[j] = s2[j] = 0;
+        const uint8_t *p = row + int64_t(m) * chunk * fstride;
+#pragma unroll 4
+        for (int t = 0; t < chunk; ++t, p += fstride) {
+            uint4 q = make_uint4(0, 0, 0, 0);
+            if (vec) {
+                q = __ldg(reinterpret_cast<const uint4 *>(p));
+            } else {
+                uint32_t x[4] = {0, 0, 0, 0};
+                for (int j = 0; j < kStdLanePixels; ++j)
+                    if (c + j < w) x[j >> 2] |= uint32_t(p[j]) << (8 * (j & 3));
+                q = make_uint4(x[0], x[1], x[2], x[3]);
+            }
+            const uint32_t wd[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+            for (int j = 0; j < kStdLanePixels; ++j) {
+                const uint32_t x = (wd[j >> 2] >> (8 * (j & 3))) & 0xFFu;
+                s1[j] += x;
+                s2[j] += x * x;
+            }
         }
-        const double var = (double(chunk) * s2 - double(s1) * s1) / (double(chunk) * chunk);
-        v[m] = float(sqrt(var > 0 ? var : 0.0));
+#pragma unroll
+        for (int j = 0; j < kStdLanePixels; ++j) {
+            const double var = (double(chunk) * s2[j] - double(s1[j]) * s1[j]) / (double(chunk) * chunk);
+            v[m * kStdPixels + j * 32 + lane] = float(sqrt(var > 0 ? var : 0.0));
+        }
     }
-    for (int a = 1; a < nchunks; ++a)   // insertion sort of a few values
-        for (int b = a; b > 0 && v[b - 1] > v[b]; --b) {
-            const float t = v[b];
-            v[b] = v[b - 1];
-            v[b - 1] = t;
+    __syncthreads();
+    for (int t = threadIdx.y * 32 + lane; t < kStdPixels; t += blockDim.x * blockDim.y) {
+        const int col = c0 + kStdLanePixels * (t & 31) + (t >> 5);
+        if (col >= w) continue;
+        float med;
+        if (nchunks <= kStdRegChunks) {
+            float x[kStdRegChunks];
+#pragma unroll
+            for (int m = 0; m < kStdRegChunks; ++m) x[m] = m < nchunks ? v[m * kStdPixels + t] : INFINITY;   // padding sorts last
+#pragma unroll
+            for (int round = 0; round < kStdRegChunks; ++round)
+#pragma unroll
+                for (int m = round & 1; m + 1 < kStdRegChunks; m += 2) {
+                    const float lo = fminf(x[m], x[m + 1]), hi = fmaxf(x[m], x[m + 1]);
+                    x[m] = lo;
+                    x[m + 1] = hi;
+                }
+            float a = 0.0f, b = 0.0f;
+#pragma unroll
+            for (int m = 0; m < kStdRegChunks; ++m) {
+                if (m == (nchunks - 1) / 2) a = x[m];
+                if (m == nchunks / 2) b = x[m];
+            }
+            med = nchunks % 2 ? b : 0.5f * (a + b);
+        } else {
+            float *col_v = v + t;   // this thread's column, kStdPixels apart
+            for (int a = 1; a < nchunks; ++a)   // insertion sort
+                for (int b = a; b > 0 && col_v[(b - 1) * kStdPixels] > col_v[b * kStdPixels]; --b) {
+                    const float x = col_v[b * kStdPixels];
+                    col_v[b * kStdPixels] = col_v[(b - 1) * kStdPixels];
+                    col_v[(b - 1) * kStdPixels] = x;
+                }
+            med = nchunks % 2 ? col_v[(nchunks / 2) * kStdPixels]
+                              : 0.5f * (col_v[(nchunks / 2 - 1) * kStdPixels] + col_v[(nchunks / 2) * kStdPixels]);
         }
-    out[i] = nchunks % 2 ? v[nchunks / 2] : 0.5f * (v[nchunks / 2 - 1] + v[nchunks / 2]);
+        out[int64_t(r) * w + col] = med;
+    }
 }
 
 __device__ __forceinline__ int scan_reflect(int i, int n) { return i < 0 ? -i - 1 : (i >= n ? 2 * n - i - 1 : i); }
@@ -143,50 +208,404 @@ __global__ void __launch_bounds__(256) sobel_kernel(const uint8_t *__restrict__ 
     out[i] = hypotf(g0, g1);
 }
 
-// mask = edge > thr && std < max_std
-__global__ void text_seed_kernel(const float *__restrict__ edge, const float *__restrict__ sd, int64_t n, float thr, float max_std,
-                                 uint8_t *__restrict__ mask)
+// ---- numpy.percentile (method 'linear') of float32 values, on the device: the two order
+// statistics around the virtual index by a radix selection over an order-preserving 32-bit key,
+// 11 + 11 + 10 bits in three passes; the percentile itself as numpy interpolates float32 data.
+
+// the state between the passes, at the start of the scratch; the two histograms follow it
+struct SelectState {
+    uint32_t prefix[2];   // the key bits resolved so far, of the lower and the upper statistic
+    uint32_t rank[2];     // their ranks among the values that share the prefix
+    uint32_t arrived;     // CTAs done with the current pass
+};
+
+// unsigned order of the keys == the order of the floats (negative below positive, NaN on top)
+__device__ __forceinline__ uint32_t order_key(float f)
 {
-    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i < n) mask[i] = edge[i] > thr && sd[i] < max_std;
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
-// one step of the binary dilation with the 3 x 3 cross (outside the image: background)
-__global__ void dilate_kernel(const uint8_t *__restrict__ in, uint8_t *__restrict__ out, int h, int w)
+__device__ __forceinline__ float key_value(uint32_t k) { return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k); }
+
+// exclusive prefix sum over a CTA of 256 threads
+__device__ __forceinline__ uint32_t cta_exclusive_sum_256(uint32_t x, uint32_t *warp_tot)
 {
-    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= int64_t(h) * w) return;
-    const int r = int(i / w), c = int(i % w);
-    out[i] = in[i] | (r > 0 && in[i - w]) | (r + 1 < h && in[i + w]) | (c > 0 && in[i - 1]) | (c + 1 < w && in[i + 1]);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = x;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= d) inc += y;
+    }
+    if (lane == 31) warp_tot[warp] = inc;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int k = 0; k < warp; ++k) before += warp_tot[k];
+    __syncthreads();
+    return before + inc - x;
 }
 
-// the background reached from the border (4-connected): outside[i] = 1 for border background;
-// each step spreads it by up to `sweeps` pixels inside a CTA's tile of rows, and flags a change
-__global__ void outside_init_kernel(const uint8_t *__restrict__ mask, uint8_t *__restrict__ outside, int h, int w)
+// One pass of the selection of the statistics of ranks lo <= hi among x[0 .. n): pass 0 counts
+// the keys' bits 31..21, pass 1 bits 20..10 of the keys that share the picked top bits, pass 2
+// bits 9..0. A CTA counts in shared memory (the equal bins of a warp added once, by
+// __match_any_sync) and adds its counts to the histograms in global memory; the last CTA to finish
+// (a ticket taken after a fence) picks each statistic's bin, narrows its rank, clears the
+// histograms for the next pass and, after pass 2, writes the percentile to *out: numpy's lerp in
+// float32, a + (b - a) * t for t < 0.5, else b - (b - a) * (1 - t), each step rounded.
+__global__ void __launch_bounds__(256) select_pass_kernel(const float *__restrict__ x, int64_t n, int pass, uint32_t lo,
+                                                          uint32_t hi, float t, SelectState *st, uint32_t *hist, float *out)
 {
-    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= int64_t(h) * w) return;
-    const int r = int(i / w), c = int(i % w);
-    outside[i] = !mask[i] && (r == 0 || c == 0 || r == h - 1 || c == w - 1);
-}
-
-__global__ void outside_step_kernel(const uint8_t *__restrict__ mask, uint8_t *__restrict__ outside, int h, int w, int *changed)
-{
-    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= int64_t(h) * w) return;
-    if (outside[i] || mask[i]) return;
-    const int r = int(i / w), c = int(i % w);
-    if ((r > 0 && outside[i - w]) || (r + 1 < h && outside[i + w]) || (c > 0 && outside[i - 1]) || (c + 1 < w && outside[i + 1])) {
-        outside[i] = 1;
-        *changed = 1;
+    constexpr int B = kSelectBins;
+    __shared__ uint32_t cnt[2][B];
+    __shared__ uint32_t warp_tot[8];
+    __shared__ uint32_t pick[2][2];
+    __shared__ int last;
+    const int shift = pass == 0 ? 21 : (pass == 1 ? 10 : 0), bins = pass == 2 ? B / 2 : B;
+    const uint32_t known = pass == 0 ? 0u : (pass == 1 ? 0xFFE00000u : 0xFFFFFC00u);
+    const uint32_t p0 = pass ? st->prefix[0] : 0u, p1 = pass ? st->prefix[1] : 0u;
+    const bool two = p0 != p1;   // the statistics took different bins: a histogram each
+    for (int i = threadIdx.x; i < 2 * B; i += blockDim.x) (&cnt[0][0])[i] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t base = int64_t(blockIdx.x) * blockDim.x; base < n; base += stride) {   // the same trips for a warp
+        const int64_t i = base + threadIdx.x;
+        const bool ok = i < n;
+        const uint32_t k = ok ? order_key(__ldg(x + i)) : 0u;
+        const uint32_t d = (k >> shift) & uint32_t(bins - 1);
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            if (s == 1 && !two) break;
+            const bool in = ok && (k & known) == (s ? p1 : p0);
+            const unsigned peers = __match_any_sync(0xffffffffu, in ? d : 0xFFFFFFFFu);
+            if (in && lane == __ffs(peers) - 1) atomicAdd(&cnt[s][d], unsigned(__popc(peers)));
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < bins; i += blockDim.x) {
+        if (cnt[0][i]) atomicAdd(hist + i, cnt[0][i]);
+        if (two && cnt[1][i]) atomicAdd(hist + B + i, cnt[1][i]);
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&st->arrived, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const uint32_t r0 = pass ? st->rank[0] : lo, r1 = pass ? st->rank[1] : hi;
+    const int per = bins / 256;   // bins per thread: 8, or 4 in pass 2
+    for (int s = 0; s < 2; ++s) {
+        const uint32_t *hs = hist + (two && s ? B : 0);
+        const uint32_t r = s ? r1 : r0;
+        uint32_t c8[8], tot = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            c8[j] = j < per ? __ldcg(hs + threadIdx.x * per + j) : 0u;
+            tot += c8[j];
+        }
+        uint32_t acc = cta_exclusive_sum_256(tot, warp_tot);
+        if (acc <= r && r < acc + tot)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (j < per && r < acc + c8[j]) {
+                    pick[s][0] = uint32_t(threadIdx.x * per + j);
+                    pick[s][1] = r - acc;
+                    break;
+                }
+                acc += c8[j];
+            }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < 2 * B; i += blockDim.x) hist[i] = 0;   // for the next pass
+    if (threadIdx.x == 0) {
+        const uint32_t q0 = p0 | (pick[0][0] << shift), q1 = p1 | (pick[1][0] << shift);
+        st->prefix[0] = q0;
+        st->prefix[1] = q1;
+        st->rank[0] = pick[0][1];
+        st->rank[1] = pick[1][1];
+        st->arrived = 0;
+        if (pass == 2) {
+            const float a = key_value(q0), b = key_value(q1), diff = __fsub_rn(b, a);
+            *out = t < 0.5f ? __fadd_rn(a, __fmul_rn(diff, t)) : __fsub_rn(b, __fmul_rn(diff, __fsub_rn(1.0f, t)));
+        }
     }
 }
 
-// the filled mask: everything not reached from the border
-__global__ void fill_kernel(const uint8_t *__restrict__ outside, uint8_t *__restrict__ out, int64_t n)
+// ---- The text mask on bit planes: bit j of word c of a row is pixel 32 c + j; a row is wpr =
+// ceil(w / 32) words, the bits past the frame's width are 0.
+
+__device__ __forceinline__ uint32_t row_bits(int c, int w)   // the bits of word c inside the frame
+{
+    const int rem = w - 32 * c;
+    return rem >= 32 ? 0xFFFFFFFFu : ((1u << rem) - 1u);
+}
+
+// mask bits = edge > *thr and sd < max_std, one warp per word (a ballot of its 32 pixels)
+__global__ void __launch_bounds__(256) text_seed_bits_kernel(const float *__restrict__ edge, const float *__restrict__ sd, int h,
+                                                             int w, int wpr, const float *__restrict__ thr, float max_std,
+                                                             uint32_t *__restrict__ bits)
+{
+    const int64_t word = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (word >= int64_t(h) * wpr) return;   // whole warps
+    const int lane = threadIdx.x & 31, r = int(word / wpr), col = 32 * int(word % wpr) + lane;
+    bool on = false;
+    if (col < w) {
+        const int64_t i = int64_t(r) * w + col;
+        on = edge[i] > *thr && sd[i] < max_std;
+    }
+    const uint32_t v = __ballot_sync(0xffffffffu, on);
+    if (lane == 0) bits[word] = v;
+}
+
+// `steps` (<= kDilateStep) steps of the binary dilation by the 3 x 3 cross (outside the frame:
+// background) for kDilateRows rows per CTA: their rows and `steps` rows either side in shared
+// memory, dilated there (the halo rows go wrong from the tile's edge inward, one row a step)
+__global__ void __launch_bounds__(256) dilate_bits_kernel(const uint32_t *__restrict__ in, uint32_t *__restrict__ out, int h,
+                                                          int w, int wpr, int steps)
+{
+    extern __shared__ uint32_t tile[];
+    const int S = kDilateRows + 2 * steps, top = blockIdx.x * kDilateRows - steps;
+    uint32_t *a = tile, *b = tile + S * wpr;
+    for (int e = threadIdx.x; e < S * wpr; e += blockDim.x) {
+        const int r = top + e / wpr;
+        a[e] = (r >= 0 && r < h) ? in[int64_t(r) * wpr + e % wpr] : 0u;
+    }
+    __syncthreads();
+    for (int k = 0; k < steps; ++k) {
+        for (int e = threadIdx.x; e < S * wpr; e += blockDim.x) {
+            const int lr = e / wpr, c = e - lr * wpr, r = top + lr;
+            uint32_t v = 0;
+            if (r >= 0 && r < h) {
+                const uint32_t m = a[e];
+                v = m | (m << 1) | (m >> 1);
+                if (c > 0) v |= a[e - 1] >> 31;
+                if (c + 1 < wpr) v |= a[e + 1] << 31;
+                if (lr > 0) v |= a[e - wpr];
+                if (lr + 1 < S) v |= a[e + wpr];
+                v &= row_bits(c, w);
+            }
+            b[e] = v;
+        }
+        __syncthreads();
+        uint32_t *x = a;
+        a = b;
+        b = x;
+    }
+    for (int e = steps * wpr + threadIdx.x; e < (steps + kDilateRows) * wpr; e += blockDim.x) {
+        const int r = top + e / wpr;
+        if (r < h) out[int64_t(r) * wpr + e % wpr] = a[e];
+    }
+}
+
+// the free pixels a seed s (inside f) reaches along f's runs toward higher bits: the carry of
+// f + s runs from each seed to the end of its run
+__device__ __forceinline__ uint32_t fill_up(uint32_t f, uint32_t s) { return (((f + s) ^ f) & f) | s; }
+__device__ __forceinline__ uint32_t fill_down(uint32_t f, uint32_t s) { return __brev(fill_up(__brev(f), __brev(s))); }
+__device__ __forceinline__ uint32_t bottom_run(uint32_t f) { return f & ~(f + 1u); }   // the run of f from bit 0
+__device__ __forceinline__ uint32_t top_run(uint32_t f) { return __brev(bottom_run(__brev(f))); }   // the run to bit 31
+
+// The horizontal sweep of a row: rightward, then leftward. A lane holds K consecutive words of a
+// segment of 32 K words (rows of more than 256 words come in several segments, the carry passed
+// along). A word filled from its own seeds gives r; its carry out is g = the run reaching the far
+// end, or the carry in when the word is all free; the carries into the lanes follow from the
+// ballots of the lanes' composite carries by one addition, and a word with a carry in adds the
+// run it enters by (the bottom run rightward, the top run leftward).
+template <int K>
+__device__ __forceinline__ bool hrow(const uint32_t *F, uint32_t *O, int64_t rb, int wpr)
+{
+    const int lane = threadIdx.x & 31;
+    bool ch = false;
+    uint32_t seg = 0;
+    for (int s0 = 0; s0 < wpr; s0 += 32 * K) {   // rightward
+        const int sw = min(32 * K, wpr - s0);
+        uint32_t f[K], o[K], r[K], G = 0, P = 1;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int j = lane * K + k;
+            f[k] = o[k] = r[k] = 0;
+            if (j < sw) {
+                f[k] = F[rb + s0 + j];
+                o[k] = O[rb + s0 + j];
+                r[k] = fill_up(f[k], o[k]);
+                const uint32_t g0 = r[k] >> 31, g1 = g0 | (f[k] == 0xFFFFFFFFu ? 1u : 0u);
+                G = g0 | (g1 & G);
+                P = g0 | (g1 & P);
+            }
+        }
+        const uint32_t g = __ballot_sync(0xffffffffu, G), p = __ballot_sync(0xffffffffu, P);
+        const uint64_t sum = uint64_t(g) + p + seg;
+        uint32_t cin = ((uint32_t(sum) ^ g ^ p) >> lane) & 1u;
+        seg = uint32_t(sum >> 32);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int j = lane * K + k;
+            if (j < sw) {
+                const uint32_t res = r[k] | (cin ? bottom_run(f[k]) : 0u);
+                cin = res >> 31;
+                if (res != o[k]) {
+                    O[rb + s0 + j] = res;
+                    ch = true;
+                }
+            }
+        }
+    }
+    __syncwarp();
+    seg = 0;
+    for (int s1 = wpr; s1 > 0; s1 -= 32 * K) {   // leftward: lanes and words from the right
+        const int s0 = max(0, s1 - 32 * K), sw = s1 - s0;
+        uint32_t f[K], o[K], r[K], G = 0, P = 1;
+#pragma unroll
+        for (int k = K - 1; k >= 0; --k) {
+            const int j = lane * K + k;
+            f[k] = o[k] = r[k] = 0;
+            if (j < sw) {
+                f[k] = F[rb + s0 + j];
+                o[k] = O[rb + s0 + j];
+                r[k] = fill_down(f[k], o[k]);
+                const uint32_t g0 = r[k] & 1u, g1 = g0 | (f[k] == 0xFFFFFFFFu ? 1u : 0u);
+                G = g0 | (g1 & G);
+                P = g0 | (g1 & P);
+            }
+        }
+        const uint32_t g = __brev(__ballot_sync(0xffffffffu, G)), p = __brev(__ballot_sync(0xffffffffu, P));
+        const uint64_t sum = uint64_t(g) + p + seg;
+        uint32_t cin = ((uint32_t(sum) ^ g ^ p) >> (31 - lane)) & 1u;
+        seg = uint32_t(sum >> 32);
+#pragma unroll
+        for (int k = K - 1; k >= 0; --k) {
+            const int j = lane * K + k;
+            if (j < sw) {
+                const uint32_t res = r[k] | (cin ? top_run(f[k]) : 0u);
+                cin = res & 1u;
+                if (res != o[k]) {
+                    O[rb + s0 + j] = res;
+                    ch = true;
+                }
+            }
+        }
+    }
+    return ch;
+}
+
+template <int K>
+__device__ __forceinline__ bool hsweep(const uint32_t *F, uint32_t *O, int h, int wpr)
+{
+    bool ch = false;
+    for (int r = threadIdx.x >> 5; r < h; r += blockDim.x >> 5) ch |= hrow<K>(F, O, int64_t(r) * wpr, wpr);
+    return ch;
+}
+
+// one 32-row block of the vertical sweep for NC columns of words at once (their scans interleave):
+// D = O | F & D_above down the block (lane order), from the carry of the block before; lane 0 of
+// the block is row r0 + lane0 and rows step by dir
+template <int NC>
+__device__ __forceinline__ bool vblock(const uint32_t *F, uint32_t *O, int h, int wpr, const int (&col)[NC], int nc, int r,
+                                       uint32_t (&carry)[NC])
+{
+    const int lane = threadIdx.x & 31;
+    bool ch = false;
+    uint32_t f[NC], o[NC], A[NC], B[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+        const bool in = q < nc && r < h && r >= 0;
+        f[q] = in ? F[int64_t(r) * wpr + col[q]] : 0u;
+        o[q] = in ? O[int64_t(r) * wpr + col[q]] : 0u;
+        A[q] = f[q];
+        B[q] = o[q];
+    }
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1)
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+            const uint32_t a2 = __shfl_up_sync(0xffffffffu, A[q], d), b2 = __shfl_up_sync(0xffffffffu, B[q], d);
+            if (lane >= d) {
+                B[q] |= A[q] & b2;
+                A[q] &= a2;
+            }
+        }
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+        const uint32_t D = B[q] | (A[q] & carry[q]);
+        carry[q] = __shfl_sync(0xffffffffu, D, 31);
+        if (q < nc && r < h && r >= 0 && D != o[q]) {
+            O[int64_t(r) * wpr + col[q]] = D;
+            ch = true;
+        }
+    }
+    return ch;
+}
+
+// The background 4-connected to the border, by one CTA of kFloodThreads threads over the bit
+// planes: in shared memory when both fit (`smem`), else in place in global memory (L1/L2). `fm`
+// holds the mask on entry and the free pixels (not mask) after; `out` gets the reached pixels.
+// It starts from the free pixels on the border and repeats a vertical and a horizontal sweep
+// until a sweep changes nothing. Vertical: a warp per column of words (two at once) carries the
+// reached bits down the column and back up, 32 rows at a time by a warp scan of
+// D = O | F & D_above. Horizontal: a warp per row (hrow) fills each word's runs from its seeds
+// by an addition's carry, and the runs across words by a ballot addition of the carries.
+// Every sweep adds a bit or ends the loop, so it ends within h * w + 1 sweeps.
+__global__ void __launch_bounds__(kFloodThreads, 1) flood_bits_kernel(uint32_t *__restrict__ fm, uint32_t *__restrict__ out, int h,
+                                                                      int w, int wpr, int smem)
+{
+    extern __shared__ uint32_t planes[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int64_t words = int64_t(h) * wpr;
+    uint32_t *F = smem ? planes : fm, *O = smem ? planes + words : out;
+    for (int64_t i = threadIdx.x; i < words; i += blockDim.x) {
+        const int r = int(i / wpr), c = int(i - int64_t(r) * wpr);
+        const uint32_t f = ~fm[i] & row_bits(c, w);
+        uint32_t edge = (c == 0 ? 1u : 0u) | (c == wpr - 1 ? 1u << ((w - 1) & 31) : 0u);
+        if (r == 0 || r == h - 1) edge = 0xFFFFFFFFu;
+        F[i] = f;
+        O[i] = f & edge;
+    }
+    __syncthreads();
+    bool go = true;
+    for (int64_t sweep = 0; go && sweep <= int64_t(h) * w; ++sweep) {
+        bool ch = false;
+        for (int c = warp; c < wpr; c += 2 * nwarp) {
+            if (c + nwarp < wpr) {   // two columns: their scans interleave
+                const int col[2] = {c, c + nwarp};
+                uint32_t carry[2] = {0u, 0u};
+                for (int r0 = 0; r0 < h; r0 += 32) ch |= vblock<2>(F, O, h, wpr, col, 2, r0 + lane, carry);   // down
+                __syncwarp();
+                carry[0] = carry[1] = 0u;
+                for (int r0 = ((h - 1) >> 5) << 5; r0 >= 0; r0 -= 32)   // up: lane 0 is the block's bottom row
+                    ch |= vblock<2>(F, O, h, wpr, col, 2, r0 + 31 - lane, carry);
+            } else {
+                const int col[1] = {c};
+                uint32_t carry[1] = {0u};
+                for (int r0 = 0; r0 < h; r0 += 32) ch |= vblock<1>(F, O, h, wpr, col, 1, r0 + lane, carry);
+                __syncwarp();
+                carry[0] = 0u;
+                for (int r0 = ((h - 1) >> 5) << 5; r0 >= 0; r0 -= 32) ch |= vblock<1>(F, O, h, wpr, col, 1, r0 + 31 - lane, carry);
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        if (wpr <= 32)
+            ch |= hsweep<1>(F, O, h, wpr);
+        else if (wpr <= 64)
+            ch |= hsweep<2>(F, O, h, wpr);
+        else if (wpr <= 128)
+            ch |= hsweep<4>(F, O, h, wpr);
+        else
+            ch |= hsweep<8>(F, O, h, wpr);
+        go = __syncthreads_or(ch);
+    }
+    if (smem)
+        for (int64_t i = threadIdx.x; i < words; i += blockDim.x) out[i] = O[i];
+}
+
+// the filled mask: every pixel the border's background does not reach
+__global__ void __launch_bounds__(256) fill_bits_kernel(const uint32_t *__restrict__ outside, int h, int w, int wpr,
+                                                        uint8_t *__restrict__ mask)
 {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = !outside[i];
+    if (i >= int64_t(h) * w) return;
+    const int r = int(i / w), c = int(i % w);
+    mask[i] = ((outside[int64_t(r) * wpr + (c >> 5)] >> (c & 31)) & 1u) ^ 1u;
 }
 
 #endif   // __CUDACC__

@@ -41,21 +41,18 @@ def frame_differences(frames, chunk=50):
     return out.cpu().numpy()
 
 
-def _percentile_like_numpy(x, q):
-    """numpy.percentile(x, q) of a float32 CUDA tensor (the 'linear' method and numpy's lerp, float32
-    result), from its two order statistics"""
+def percentile(x, q):
+    """numpy.percentile(x, q) (method 'linear') of a float32 CUDA tensor, as numpy computes it for
+    float32 data; a float32 scalar. The selection runs on the device (csrc/scans.cuh)."""
     import torch
-    v = x.flatten()
-    n = v.numel()
-    idx = q / 100.0 * (n - 1)
-    lo = int(np.floor(idx))
-    hi = min(lo + 1, n - 1)
-    t = idx - lo
-    a = np.float32(torch.kthvalue(v, lo + 1).values.item())
-    b = np.float32(torch.kthvalue(v, hi + 1).values.item())
-    diff = np.float32(b - a)
-    r = a + diff * t if t < 0.5 else b - diff * (1 - t)
-    return np.float32(r)
+    if not (isinstance(x, torch.Tensor) and x.is_cuda and x.dtype == torch.float32):
+        raise TypeError('framecor: percentile takes a float32 CUDA tensor')
+    v = x.contiguous()
+    out = torch.empty(1, dtype=torch.float32, device=v.device)
+    scratch = torch.empty(_lib.PERCENTILE_SCRATCH, dtype=torch.uint8, device=v.device)
+    _check(_lib.lib().b200_percentile_f32_device(v.data_ptr(), v.numel(), float(q), out.data_ptr(), scratch.data_ptr(),
+                                                 torch.cuda.current_stream().cuda_stream))
+    return np.float32(out.item())
 
 
 def text_mask(frames, start, nframes=150, chunk=10, edge_percentile=90, max_std=1.5, dilate=4):
@@ -76,10 +73,8 @@ def text_mask(frames, start, nframes=150, chunk=10, edge_percentile=90, max_std=
     ref = _device(frames, start, start + 1)
     edge = torch.empty((h, w), dtype=torch.float32, device='cuda')
     _check(_lib.lib().b200_sobel_device(ref.data_ptr(), h, w, w, edge.data_ptr(), stream))
-    thr = _percentile_like_numpy(edge, edge_percentile)
     mask = torch.empty((h, w), dtype=torch.uint8, device='cuda')
-    scratch = torch.empty(2 * h * w, dtype=torch.uint8, device='cuda')
-    flag = torch.empty(1, dtype=torch.int32, device='cuda')
-    _check(_lib.lib().b200_text_mask_device(edge.data_ptr(), sd.data_ptr(), h, w, float(thr), float(max_std), int(dilate),
-                                            mask.data_ptr(), scratch.data_ptr(), flag.data_ptr(), stream))
+    scratch = torch.empty(_lib.lib().b200_text_mask_scratch_bytes(h, w), dtype=torch.uint8, device='cuda')
+    _check(_lib.lib().b200_text_mask_device(edge.data_ptr(), sd.data_ptr(), h, w, float(edge_percentile), float(max_std),
+                                            int(dilate), mask.data_ptr(), scratch.data_ptr(), scratch.numel(), stream))
     return mask.cpu().numpy().astype(bool)

@@ -76,3 +76,122 @@ def test_frame_differences_any_alignment(width, offset):
     exact = np.array([np.abs(f[k + 1].astype(np.int64) - f[k].astype(np.int64)).sum() for k in range(n - 1)])
     assert np.array_equal(sums.cpu().numpy(), exact)
     np.testing.assert_array_equal(out.cpu().numpy(), oracle.frame_differences(f))
+
+
+def test_text_mask_arguments_checked_before_any_launch():
+    """Bad arguments come back as EINVAL from the C ABI without touching a device; the scratch size."""
+    from slipcam_b200 import _lib
+    lib = _lib.lib()
+    assert lib.b200_text_mask_scratch_bytes(720, 1280) == _lib.PERCENTILE_SCRATCH + 2 * 720 * 40 * 4
+    assert lib.b200_text_mask_scratch_bytes(0, 5) == 0
+    assert lib.b200_percentile_f32_device(None, 10, 50.0, None, None, None) == _lib.EINVAL
+    assert lib.b200_percentile_f32_device(1, 10, 100.5, 1, 1, None) == _lib.EINVAL
+    assert lib.b200_percentile_f32_device(1, 10, float('nan'), 1, 1, None) == _lib.EINVAL
+    assert lib.b200_percentile_f32_device(1, 0, 50.0, 1, 1, None) == _lib.EINVAL
+    assert lib.b200_text_mask_device(1, 1, 4, 4, 90.0, 1.5, 4, 1, 1, 10, None) == _lib.EINVAL   # scratch too small
+    assert lib.b200_text_mask_device(1, 1, 4, 40000, 90.0, 1.5, 4, 1, 1, 1 << 30, None) == _lib.EINVAL   # too wide
+
+
+@pytest.mark.gpu
+def test_b200_percentile_matches_numpy():
+    """numpy.percentile of float32 data, bit for bit: negatives, ties, constant data, one value,
+    q at 0 and 100, and a 720p edge map."""
+    import torch
+    from slipcam_b200 import scans
+    rng = np.random.default_rng(11)
+    cases = []
+    for n in (1, 2, 3, 17, 1000, 4097, 100_003):
+        x = (rng.standard_normal(n) * 50).astype(np.float32)
+        cases += [x, np.round(x).astype(np.float32), np.abs(x), np.full(n, 2.5, np.float32)]
+    g = golden()['frames'][0].astype(np.float32)
+    cases.append(oracle._sobel_magnitude(g))
+    cases.append((rng.random(720 * 1280) * 300).astype(np.float32))
+    for x in cases:
+        t = torch.as_tensor(x).cuda()
+        for q in (0, 100, 90, 85, 50, 12.5, 99.9, 33.3):
+            assert scans.percentile(t, q) == np.percentile(x, q), (x.size, q)
+
+
+def _spiral(h, w):
+    m = np.zeros((h, w), bool)
+    t, l, b, r, k = 2, 2, h - 3, w - 3, 0
+    while t < b and l < r:
+        m[t, l:r + 1] = m[t:b + 1, r] = m[b, l:r + 1] = True
+        m[t + 2:b + 1, l] = True
+        if k % 2:
+            m[t, l + 1] = False
+        t, l, b, r, k = t + 2, l + 2, b - 2, r - 2, k + 1
+    return m
+
+
+def _mask_device(edge, sd, q, max_std, dilate):
+    import torch
+    from slipcam_b200 import _lib
+    h, w = edge.shape
+    lib = _lib.lib()
+    e, s = torch.as_tensor(edge).cuda(), torch.as_tensor(sd).cuda()
+    mask = torch.empty((h, w), dtype=torch.uint8, device='cuda')
+    scratch = torch.empty(lib.b200_text_mask_scratch_bytes(h, w), dtype=torch.uint8, device='cuda')
+    rc = lib.b200_text_mask_device(e.data_ptr(), s.data_ptr(), h, w, float(q), float(max_std), dilate, mask.data_ptr(),
+                                   scratch.data_ptr(), scratch.numel(), torch.cuda.current_stream().cuda_stream)
+    assert rc == _lib.OK
+    return mask.cpu().numpy().astype(bool)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('h,w', [(1, 1), (1, 70), (45, 1), (37, 70), (64, 96), (50, 129), (200, 333), (9, 2049),
+                                 (6, 9000)])
+def test_b200_mask_from_maps_random(h, w):
+    """The threshold, dilation and hole filling on the device against the oracle (scipy labels):
+    random seed masks of several densities, dilation 0, 1, 4 and 11 (two launches of the tile
+    dilation), rows of several words per lane in the horizontal sweep (2049 pixels) and wider than
+    one of its segments (9000 pixels)."""
+    rng = np.random.default_rng(h * 1000 + w)
+    for dens in (0.02, 0.1, 0.3):
+        edge = (rng.random((h, w)) * 100).astype(np.float32)
+        sd = np.where(rng.random((h, w)) < 1 - dens, 5.0, 0.5).astype(np.float32)
+        for q, dilate in ((90, 4), (50, 0), (99, 1), (0, 11)):
+            got = _mask_device(edge, sd, q, 1.5, dilate)
+            assert np.array_equal(got, oracle.mask_from_maps(edge, sd, q, 1.5, dilate)), (dens, q, dilate)
+
+
+@pytest.mark.gpu
+def test_b200_mask_fills_spirals_and_rings():
+    """Shapes the sweeps need many rounds for: nested spirals (a corridor that turns at every ring)
+    and a ring inside a ring."""
+    for h, w in ((41, 67), (120, 300), (257, 129), (20, 1300)):
+        m = _spiral(h, w)
+        edge, sd = np.where(m, 100.0, 1.0).astype(np.float32), np.zeros((h, w), np.float32)
+        q = 100.0 * (1 - m.mean()) - 1e-3
+        got = _mask_device(edge, sd, q, 1.5, 0)
+        assert np.array_equal(got, oracle.mask_from_maps(edge, sd, q, 1.5, 0))
+    m = np.zeros((90, 140), bool)
+    m[5, 5:130] = m[80, 5:130] = True
+    m[5:81, 5] = m[5:81, 129] = True
+    m[20, 20:100] = m[60, 20:100] = True
+    m[20:61, 20] = m[20:61, 99] = True
+    m[20, 50] = False   # the inner ring opens into the outer ring's hole: both still enclosed
+    edge, sd = np.where(m, 100.0, 1.0).astype(np.float32), np.zeros(m.shape, np.float32)
+    got = _mask_device(edge, sd, 100.0 * (1 - m.mean()) - 1e-3, 1.5, 0)
+    assert got[40, 60] and got[70, 60] and not got[2, 2]
+    assert np.array_equal(got, oracle.mask_from_maps(edge, sd, 100.0 * (1 - m.mean()) - 1e-3, 1.5, 0))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('nchunks,chunk,width', [(15, 10, 1280), (1, 3, 77), (2, 5, 130), (4, 2, 128), (17, 2, 101),
+                                                 (64, 1, 33)])
+def test_b200_chunk_std_median(nchunks, chunk, width):
+    """The temporal median of the chunks' deviations against the oracle: odd and even chunk counts,
+    the register sort (up to 16 chunks) and the shared-memory one (17 and 64), widths that are not
+    a multiple of 4 (the byte path)."""
+    import torch
+    from slipcam_b200 import _lib
+    rng = np.random.default_rng(nchunks * 7 + width)
+    h = 23
+    f = rng.integers(0, 256, (nchunks * chunk, h, width), dtype=np.uint8)
+    f[:, :5] = 128 + rng.integers(0, 2, (nchunks * chunk, 5, width), dtype=np.uint8)   # steady rows
+    out = torch.empty((h, width), dtype=torch.float32, device='cuda')
+    rc = _lib.lib().b200_chunk_std_median_device(torch.as_tensor(f).cuda().data_ptr(), nchunks, chunk, h, width, width,
+                                                 out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert rc == _lib.OK
+    assert np.array_equal(out.cpu().numpy(), oracle.chunk_std_median(f, 0, nchunks * chunk, chunk))
