@@ -1089,13 +1089,26 @@ int b200_chunk_std_median_device(const uint8_t *frames, int nchunks, int chunk, 
         rows = 1;
         step = cols;
     }
-    const size_t smem = size_t(nchunks) * kStdPixels * sizeof(float);
-    if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(chunk_std_median_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+    // the numerators fit 32 bits while chunk <= 513 (chunk^2 x 127.5^2 < 2^32)
+    const bool narrow = chunk <= 513;
+    const size_t smem = size_t(nchunks) * kStdPixels * (narrow ? 4 : 8);
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
         return B200_ERUNTIME;
+    if (smem > size_t(optin)) return B200_EINVAL;
+    const void *kernel = narrow ? reinterpret_cast<const void *>(chunk_std_median_kernel<uint32_t>)
+                                : reinterpret_cast<const void *>(chunk_std_median_kernel<uint64_t>);
+    if (smem > 48 * 1024 && cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+        return B200_ERUNTIME;
+    const dim3 grid(unsigned((cols + kStdPixels - 1) / kStdPixels), unsigned(rows));
     const dim3 block(32, unsigned(std::min(nchunks, kStdRegChunks)));
-    chunk_std_median_kernel<<<dim3(unsigned((cols + kStdPixels - 1) / kStdPixels), unsigned(rows)), block, smem,
-                              static_cast<cudaStream_t>(stream)>>>(frames, fstride, step, rows, cols, chunk, nchunks, out);
+    if (narrow)
+        chunk_std_median_kernel<uint32_t><<<grid, block, smem, static_cast<cudaStream_t>(stream)>>>(frames, fstride, step, rows,
+                                                                                                  cols, chunk, nchunks, out);
+    else
+        chunk_std_median_kernel<uint64_t><<<grid, block, smem, static_cast<cudaStream_t>(stream)>>>(frames, fstride, step, rows,
+                                                                                                  cols, chunk, nchunks, out);
     return cudaGetLastError() == cudaSuccess ? B200_OK : B200_ERUNTIME;
 }
 

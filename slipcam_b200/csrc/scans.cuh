@@ -104,90 +104,108 @@ __global__ void __launch_bounds__(256) frame_diff_kernel(const uint8_t *__restri
 
 // per pixel: the population standard deviation of each chunk of `chunk` frames (exact integer
 // sums, the root in float), then their median over nchunks (the mean of the two middle values
-// when nchunks is even, as numpy.median). A CTA takes kStdPixels pixels of a row (a frame whose
-// rows are contiguous comes as one long row), 16 per lane in one 16-byte load where aligned;
-// warp y sums chunks y, y + blockDim.y, ... so the loads of every chunk are in flight together.
-// The deviations meet in shared memory (chunk m's slot t holds the lane's pixel t / 32 of lane
-// t % 32) and thread t sorts slot t's column: in registers by odd-even transposition up to
-// kStdRegChunks chunks, in place in shared memory above.
-constexpr int kStdLanePixels = 16;
+// when nchunks is even, as numpy.median). The deviation float(sqrt(num / chunk^2)) (float64
+// division and root) is non-decreasing in the exact numerator num = chunk * sum x^2 - (sum x)^2,
+// so the chunks are ordered by num and only the middle one or two become deviations. A CTA takes
+// kStdPixels pixels of a row (a frame whose rows are contiguous comes as one long row), 8 per
+// lane in one 8-byte load where aligned; warp y sums chunks y, y + blockDim.y, ..., a batch of
+// kStdBatch frames' loads in flight together. The numerators meet in shared memory (chunk m's slot t
+// holds the pixel t / 32 of lane t % 32) and thread t orders slot t's column: up to kStdRegChunks
+// chunks by Batcher's odd-even merge network in registers, above that by insertion in place.
+// NumT: uint32_t while chunk <= 513 (num < 2^32), else uint64_t.
+constexpr int kStdLanePixels = 8;
 constexpr int kStdPixels = 32 * kStdLanePixels;
 constexpr int kStdRegChunks = 16;
+constexpr int kStdBatch = 16;   // frames of a chunk whose loads are in flight together
 
+__device__ __forceinline__ float chunk_std(uint64_t num, int chunk)
+{
+    return float(sqrt(double(num) / (double(chunk) * chunk)));
+}
+
+template <typename NumT>
 __global__ void __launch_bounds__(512, 2) chunk_std_median_kernel(const uint8_t *__restrict__ frames, int64_t fstride, int pitch,
                                                                     int h, int w, int chunk, int nchunks, float *__restrict__ out)
 {
-    extern __shared__ float v[];   // [nchunks][kStdPixels]
+    extern __shared__ __align__(8) unsigned char std_smem[];
+    NumT *v = reinterpret_cast<NumT *>(std_smem);   // [nchunks][kStdPixels]
     const int r = blockIdx.y, c0 = blockIdx.x * kStdPixels, lane = threadIdx.x;
     const int c = c0 + kStdLanePixels * lane;
     const uint8_t *row = frames + int64_t(r) * pitch + c;
-    const bool vec = ((reinterpret_cast<uintptr_t>(row) | uintptr_t(fstride)) & 15) == 0 && c + kStdLanePixels <= w;
+    const bool vec = ((reinterpret_cast<uintptr_t>(row) | uintptr_t(fstride)) & 7) == 0 && c + kStdLanePixels <= w;
     for (int m = threadIdx.y; m < nchunks; m += blockDim.y) {
         uint32_t s1[kStdLanePixels], s2[kStdLanePixels];
 #pragma unroll
         for (int j = 0; j < kStdLanePixels; ++j) s1[j] = s2[j] = 0;
         const uint8_t *p = row + int64_t(m) * chunk * fstride;
-#pragma unroll 4
-        for (int t = 0; t < chunk; ++t, p += fstride) {
-            uint4 q = make_uint4(0, 0, 0, 0);
-            if (vec) {
-                q = __ldg(reinterpret_cast<const uint4 *>(p));
-            } else {
-                uint32_t x[4] = {0, 0, 0, 0};
-                for (int j = 0; j < kStdLanePixels; ++j)
-                    if (c + j < w) x[j >> 2] |= uint32_t(p[j]) << (8 * (j & 3));
-                q = make_uint4(x[0], x[1], x[2], x[3]);
-            }
-            const uint32_t wd[4] = {q.x, q.y, q.z, q.w};
+        if (vec) {
+            for (int t0 = 0; t0 < chunk; t0 += kStdBatch, p += kStdBatch * fstride) {
+                uint2 q[kStdBatch];   // the batch's loads all issue before any is used
 #pragma unroll
-            for (int j = 0; j < kStdLanePixels; ++j) {
-                const uint32_t x = (wd[j >> 2] >> (8 * (j & 3))) & 0xFFu;
-                s1[j] += x;
-                s2[j] += x * x;
+                for (int k = 0; k < kStdBatch; ++k)
+                    q[k] = t0 + k < chunk ? __ldg(reinterpret_cast<const uint2 *>(p + k * fstride)) : make_uint2(0, 0);
+#pragma unroll
+                for (int k = 0; k < kStdBatch; ++k)
+#pragma unroll
+                    for (int j = 0; j < kStdLanePixels; ++j) {
+                        const uint32_t x = __byte_perm(j < 4 ? q[k].x : q[k].y, 0u, 0x4440u | unsigned(j & 3));
+                        s1[j] += x;
+                        s2[j] += x * x;
+                    }
             }
+        } else {   // unaligned rows or the row's last pixels: byte loads
+            for (int t = 0; t < chunk; ++t, p += fstride)
+#pragma unroll
+                for (int j = 0; j < kStdLanePixels; ++j) {
+                    const uint32_t x = c + j < w ? p[j] : 0u;
+                    s1[j] += x;
+                    s2[j] += x * x;
+                }
         }
 #pragma unroll
-        for (int j = 0; j < kStdLanePixels; ++j) {
-            const double var = (double(chunk) * s2[j] - double(s1[j]) * s1[j]) / (double(chunk) * chunk);
-            v[m * kStdPixels + j * 32 + lane] = float(sqrt(var > 0 ? var : 0.0));
-        }
+        for (int j = 0; j < kStdLanePixels; ++j)
+            v[m * kStdPixels + j * 32 + lane] = NumT(uint64_t(chunk) * s2[j] - uint64_t(s1[j]) * s1[j]);
     }
     __syncthreads();
     for (int t = threadIdx.y * 32 + lane; t < kStdPixels; t += blockDim.x * blockDim.y) {
         const int col = c0 + kStdLanePixels * (t & 31) + (t >> 5);
         if (col >= w) continue;
-        float med;
+        NumT lo = 0, hi = 0;   // the numerators of ranks (nchunks - 1) / 2 and nchunks / 2
         if (nchunks <= kStdRegChunks) {
-            float x[kStdRegChunks];
+            NumT x[kStdRegChunks];
 #pragma unroll
-            for (int m = 0; m < kStdRegChunks; ++m) x[m] = m < nchunks ? v[m * kStdPixels + t] : INFINITY;   // padding sorts last
+            for (int m = 0; m < kStdRegChunks; ++m) x[m] = m < nchunks ? v[m * kStdPixels + t] : ~NumT(0);   // padding sorts last
 #pragma unroll
-            for (int round = 0; round < kStdRegChunks; ++round)
+            for (int p = 1; p < kStdRegChunks; p <<= 1)
 #pragma unroll
-                for (int m = round & 1; m + 1 < kStdRegChunks; m += 2) {
-                    const float lo = fminf(x[m], x[m + 1]), hi = fmaxf(x[m], x[m + 1]);
-                    x[m] = lo;
-                    x[m + 1] = hi;
-                }
-            float a = 0.0f, b = 0.0f;
+                for (int k = p; k >= 1; k >>= 1)
+#pragma unroll
+                    for (int j = k % p; j + k < kStdRegChunks; j += 2 * k)
+#pragma unroll
+                        for (int i = 0; i < k; ++i)
+                            if (i + j + k < kStdRegChunks && (i + j) / (2 * p) == (i + j + k) / (2 * p)) {
+                                const NumT a = x[i + j], b = x[i + j + k];
+                                x[i + j] = min(a, b);
+                                x[i + j + k] = max(a, b);
+                            }
 #pragma unroll
             for (int m = 0; m < kStdRegChunks; ++m) {
-                if (m == (nchunks - 1) / 2) a = x[m];
-                if (m == nchunks / 2) b = x[m];
+                if (m == (nchunks - 1) / 2) lo = x[m];
+                if (m == nchunks / 2) hi = x[m];
             }
-            med = nchunks % 2 ? b : 0.5f * (a + b);
         } else {
-            float *col_v = v + t;   // this thread's column, kStdPixels apart
+            NumT *col_v = v + t;   // this thread's column, kStdPixels apart
             for (int a = 1; a < nchunks; ++a)   // insertion sort
                 for (int b = a; b > 0 && col_v[(b - 1) * kStdPixels] > col_v[b * kStdPixels]; --b) {
-                    const float x = col_v[b * kStdPixels];
+                    const NumT x = col_v[b * kStdPixels];
                     col_v[b * kStdPixels] = col_v[(b - 1) * kStdPixels];
                     col_v[(b - 1) * kStdPixels] = x;
                 }
-            med = nchunks % 2 ? col_v[(nchunks / 2) * kStdPixels]
-                              : 0.5f * (col_v[(nchunks / 2 - 1) * kStdPixels] + col_v[(nchunks / 2) * kStdPixels]);
+            lo = col_v[((nchunks - 1) / 2) * kStdPixels];
+            hi = col_v[(nchunks / 2) * kStdPixels];
         }
-        out[int64_t(r) * w + col] = med;
+        const float b = chunk_std(hi, chunk);
+        out[int64_t(r) * w + col] = nchunks % 2 ? b : 0.5f * (chunk_std(lo, chunk) + b);
     }
 }
 
