@@ -7,7 +7,7 @@ numpy array (memory-mapped or not; copied to the GPU in chunks) or a CUDA tensor
 
 import numpy as np
 
-from . import _lib
+from . import _lib, _stage
 
 
 def _check(rc):
@@ -32,12 +32,27 @@ def frame_differences(frames, chunk=50):
     h, w = frames.shape[1:]
     out = torch.empty(n - 1, dtype=torch.float32, device='cuda')
     sums = torch.empty(n - 1, dtype=torch.int64, device='cuda')
-    stream = torch.cuda.current_stream().cuda_stream
-    for a in range(0, n - 1, chunk):   # chunk + 1 frames: the pairs (a, a + 1) .. (b - 2, b - 1)
-        b = min(a + chunk + 1, n)
-        f = _device(frames, a, b)
-        _check(_lib.lib().b200_frame_diff_device(f.data_ptr(), b - a, h, w, w, out[a:].data_ptr(), sums[a:].data_ptr(),
-                                                 stream))
+    stream = torch.cuda.current_stream()
+    lib = _lib.lib()
+
+    def scan(f, a, m):
+        _check(lib.b200_frame_diff_device(f.data_ptr(), m, h, w, w, out[a:].data_ptr(), sums[a:].data_ptr(),
+                                          stream.cuda_stream))
+    if isinstance(frames, torch.Tensor):
+        for a in range(0, n - 1, chunk):   # chunk + 1 frames: the pairs (a, a + 1) .. (b - 2, b - 1)
+            b = min(a + chunk + 1, n)
+            scan(_device(frames, a, b), a, b - a)
+        return out.cpu().numpy()
+    # host frames: staged through pinned memory, the copy of a chunk overlapping the scan of the last
+    C = min(chunk, n - 1) + 1
+    up = _stage.Uploader((h, w), C, stream.device)
+    bufs = [torch.empty((C, h, w), dtype=torch.uint8, device='cuda') for _ in range(2)]
+    done = [None, None]
+    for i, a in enumerate(range(0, n - 1, chunk)):
+        b, k = min(a + chunk + 1, n), i % 2
+        stream.wait_event(up.put(frames[a:b], bufs[k][:b - a], after=done[k]))
+        scan(bufs[k], a, b - a)
+        done[k] = stream.record_event()
     return out.cpu().numpy()
 
 
@@ -67,10 +82,18 @@ def text_mask(frames, start, nframes=150, chunk=10, edge_percentile=90, max_std=
     if not starts:
         raise ValueError('framecor: no complete chunk of frames for the text mask')
     stream = torch.cuda.current_stream().cuda_stream
-    f = _device(frames, starts[0], starts[-1] + chunk)
+    if isinstance(frames, torch.Tensor):
+        f = _device(frames, starts[0], starts[-1] + chunk)
+    else:   # staged through pinned memory, 32 frames at a time
+        f = torch.empty((starts[-1] + chunk - starts[0], h, w), dtype=torch.uint8, device='cuda')
+        up = _stage.Uploader((h, w), 32, f.device)
+        ev = None
+        for k in range(0, len(f), 32):
+            ev = up.put(frames[starts[0] + k:starts[0] + min(k + 32, len(f))], f[k:k + 32])
+        torch.cuda.current_stream().wait_event(ev)
     sd = torch.empty((h, w), dtype=torch.float32, device='cuda')
     _check(_lib.lib().b200_chunk_std_median_device(f.data_ptr(), len(starts), chunk, h, w, w, sd.data_ptr(), stream))
-    ref = _device(frames, start, start + 1)
+    ref = f[start - starts[0]:start - starts[0] + 1]
     edge = torch.empty((h, w), dtype=torch.float32, device='cuda')
     _check(_lib.lib().b200_sobel_device(ref.data_ptr(), h, w, w, edge.data_ptr(), stream))
     mask = torch.empty((h, w), dtype=torch.uint8, device='cuda')

@@ -28,7 +28,7 @@ import ctypes
 
 import numpy as np
 
-from . import _lib, framecor
+from . import _lib, _stage, framecor
 
 
 def apply(params, x, y):
@@ -77,15 +77,6 @@ def _keep(ref, text, yc, xc, half):
             keep[i, j] = (not text[y - half:y + half, x - half:x + half].any()
                           and refimg[y - half:y + half, x - half:x + half].std() > 2)
     return keep
-
-
-def _host_range(frames, lo, hi):
-    """frames[lo:hi] as a C-contiguous, writable numpy array (a copy only when it is not one already:
-    memory-mapped, strided or read-only input)"""
-    src = frames[lo:hi]
-    if not (isinstance(src, np.ndarray) and src.flags.c_contiguous and src.flags.writeable):
-        src = np.array(src, np.uint8, order='C')
-    return src
 
 
 def _runs(order, chunk):
@@ -172,30 +163,31 @@ class CoarseTracker:
                             track(rev.data_ptr(), len(run), at, c == 0)
                         at += len(run)
             elif order:
-                # each chunk copied straight from the caller's array on a side stream (a backward
-                # chunk reversed on the device), the copy of chunk k + 1 overlapping the tracking of
-                # chunk k; two device buffers, each reused once its chunk is tracked
+                # each chunk staged through pinned memory on a side stream (a backward chunk reversed
+                # on the device), the copy of chunk k + 1 overlapping the tracking of chunk k; two
+                # device buffers, each reused once its chunk is tracked
                 C = min(chunk, len(order))
                 devb = [torch.empty((C, h, w), dtype=torch.uint8, device=dev) for _ in range(2)]
-                copy = torch.cuda.Stream(dev)
+                rev = torch.empty((C, h, w), dtype=torch.uint8, device=dev)
+                up = _stage.Uploader((h, w), C, dev)
                 done = [None, None]
                 b = 0
                 for frames_in_order in passes:
                     for c, run in enumerate(_runs(frames_in_order, C)):
-                        lo, hi = min(run[0], run[-1]), max(run[0], run[-1]) + 1
-                        src = torch.from_numpy(_host_range(frames, lo, hi))
-                        with torch.cuda.stream(copy):
-                            if done[b] is not None:
-                                copy.wait_event(done[b])   # the chunk before last is tracked
-                            if run[0] <= run[-1]:
-                                devb[b][:len(run)].copy_(src, non_blocking=True)
-                            else:
-                                devb[b][:len(run)].copy_(src.to(dev, non_blocking=True).flip(0))
-                            ready = copy.record_event()
+                        lo, hi, m = min(run[0], run[-1]), max(run[0], run[-1]) + 1, len(run)
+                        if run[0] <= run[-1]:
+                            ready = up.put(frames[lo:hi], devb[b][:m], after=done[b])
+                        else:
+                            up.put(frames[lo:hi], rev[:m])
+                            with torch.cuda.stream(up.stream):
+                                if done[b] is not None:
+                                    up.stream.wait_event(done[b])   # the chunk before last is tracked
+                                devb[b][:m].copy_(rev[:m].flip(0))
+                                ready = up.stream.record_event()
                         stream.wait_event(ready)
-                        track(devb[b].data_ptr(), len(run), at, c == 0)
+                        track(devb[b].data_ptr(), m, at, c == 0)
                         done[b] = stream.record_event()
-                        at += len(run)
+                        at += m
                         b ^= 1
             if order:
                 params[order] = out.cpu().numpy()
@@ -313,40 +305,23 @@ class Stabilizer:
                 if n:
                     run(f, n, 0, out)
                 return out, union.bool()
-            # two sets of device buffers; chunk k + 1 is copied in (straight from the caller's array,
-            # on a side stream) and warped while chunk k is copied out into the result (on another)
+            # two sets of device buffers; chunk k + 1 is staged in through pinned memory (on a side
+            # stream) and warped while chunk k is staged out into the result (on another)
             out = np.empty((n, h, w), np.uint8)
             C = max(1, min(chunk, n))
             dev_in = [torch.empty((C, h, w), dtype=torch.uint8, device=dev) for _ in range(2)]
             dev_out = [torch.empty((C, h, w), dtype=torch.uint8, device=dev) for _ in range(2)]
-            copy_in, copy_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
-            chunks = [(k0, min(C, n - k0)) for k0 in range(0, n, C)]
-            done = [None, None]
-
-            def start(c):
-                b, (k0, m) = c % 2, chunks[c]
-                src = torch.from_numpy(_host_range(frames, k0, k0 + m))
-                with torch.cuda.stream(copy_in):
-                    if done[b] is not None:
-                        copy_in.wait_event(done[b])   # chunk c - 2 no longer reads dev_in[b]
-                    dev_in[b][:m].copy_(src, non_blocking=True)
-                    ready = copy_in.record_event()
-                stream.wait_event(ready)
+            up, down = _stage.Uploader((h, w), C, dev), _stage.Downloader((h, w), C, dev)
+            read_in, read_out = [None, None], [None, None]
+            for c, k0 in enumerate(range(0, n, C)):
+                b, m = c % 2, min(C, n - k0)
+                stream.wait_event(up.put(frames[k0:k0 + m], dev_in[b][:m], after=read_in[b]))
+                if read_out[b] is not None:
+                    stream.wait_event(read_out[b])   # chunk c - 2 is out of dev_out[b]
                 run(dev_in[b], m, k0, dev_out[b])
-                done[b] = stream.record_event()
-
-            def finish(c):
-                b, (k0, m) = c % 2, chunks[c]
-                with torch.cuda.stream(copy_out):
-                    copy_out.wait_event(done[b])
-                    torch.from_numpy(out[k0:k0 + m]).copy_(dev_out[b][:m])   # returns when copied
-            if chunks:
-                start(0)
-            for c in range(1, len(chunks)):
-                start(c)
-                finish(c - 1)
-            if chunks:
-                finish(len(chunks) - 1)
+                read_in[b] = stream.record_event()
+                read_out[b] = down.get(dev_out[b][:m], out[k0:k0 + m], after=read_in[b])
+            down.flush()
             return out, union.cpu().numpy().astype(bool)
 
 
