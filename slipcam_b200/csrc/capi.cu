@@ -348,7 +348,7 @@ struct b200_handle {
     DevBuf<float> d_dinv;
     Slot slot[2];
     bool slots_ready = false;    // the slots are allocated (ensure_slots)
-    DevBuf<uint32_t> d_csat;     // coarse tracking: the second set of tables
+    DevBuf<uint32_t> d_csat;     // coarse tracking: two sets of tables of kCoarseGroup frames
     DevBuf<int64_t> d_csat2;
     DevBuf<float> d_cdinv;
     DevBuf<uint16_t> d_dtab;     // the FP16 DFT matrices of the tensor-core form
@@ -409,6 +409,21 @@ struct b200_handle {
             CK(cudaMemcpy(d_tmaps.p, maps, sizeof(maps), cudaMemcpyHostToDevice));
         }
         slots_ready = true;
+    }
+
+    // the device path's tables for `group` frames (and the TMA map of its denominators), allocated
+    // by the first device-path call: coarse tracking and the host path never pay for them
+    void ensure_tables()
+    {
+        if (d_sat.p) return;
+        const size_t G = size_t(group);
+        d_sat.alloc(G * sat_size());
+        d_sat2.alloc(G * sat_size());
+        d_dinv.alloc(G * dinv_size());
+        if (tc_ok) {
+            const CUtensorMap m = dinv_map(d_dinv.p, height, width, dpitch(), int(G), M);
+            CK(cudaMemcpy(d_tmaps.p + 2, &m, sizeof(m), cudaMemcpyHostToDevice));
+        }
     }
 
     // the tables and the correlation of nf frames (device memory) on stream s
@@ -714,16 +729,8 @@ int b200_create(const b200_params *p, int device, b200_handle **out)
             CK(cudaMemcpy(h->d_dtab.p, dt.data(), dt.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
         }
         if (N == kBigN) h->d_big.alloc(size_t(num_sms()) * big_scratch_per_cta(L, h->M));
-        const size_t G = size_t(h->group);
-        h->d_sat.alloc(G * h->sat_size());
-        h->d_sat2.alloc(G * h->sat_size());
-        h->d_dinv.alloc(G * h->dinv_size());
-        if (h->tc_ok) {
-            // the maps of the two slots are written when the slots are allocated
-            h->d_tmaps.alloc(3);
-            const CUtensorMap m = dinv_map(h->d_dinv.p, h->height, h->width, h->dpitch(), int(G), h->M);
-            CK(cudaMemcpy(h->d_tmaps.p + 2, &m, sizeof(m), cudaMemcpyHostToDevice));
-        }
+        // the maps of the two slots and of the device path's table are written when those are allocated
+        if (h->tc_ok) h->d_tmaps.alloc(3);
         *out = h;
         g_create_error.clear();
         return B200_OK;
@@ -869,6 +876,7 @@ static int correlate_device(b200_handle *h, const uint8_t *frames, int n, int pi
         if (!frames || pitch < h->width || !offset || !peak || !snr || !cov) fail(B200_EINVAL, "null input or output, or a pitch below the width");
         CK(cudaSetDevice(h->device));
         cudaStream_t s = static_cast<cudaStream_t>(stream);
+        h->ensure_tables();
         // groups of equal size, at most h->group frames
         const int G = (n + (n + h->group - 1) / h->group - 1) / ((n + h->group - 1) / h->group), nwin = h->nwin;
         const int64_t fstride = int64_t(pitch) * h->height;
@@ -1184,11 +1192,32 @@ int b200_text_mask_device(const float *edge, const float *sd, int height, int wi
                                                                                                  steps);
         std::swap(m, o);
     }
-    // the hole filling's two planes in shared memory when they fit (720p: 225 KB)
     int dev = 0, optin = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
         return B200_ERUNTIME;
+    // the hole filling: a cluster of CTAs holding bands of rows when a band fits a CTA's shared
+    // memory (720p: 31 KB, 2160 x 3840: 273 KB, too much) and the cluster can be placed
+    const int hb = ((height + kFloodCluster - 1) / kFloodCluster + 31) / 32 * 32;
+    const size_t band_bytes = (2 * size_t(hb) * wpr + 4 * size_t(wpr)) * 4 + 2 * sizeof(int);
+    if (band_bytes <= size_t(optin)) {
+        if (band_bytes > 48 * 1024 &&
+            cudaFuncSetAttribute(flood_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(band_bytes)) !=
+                cudaSuccess)
+            return B200_ERUNTIME;
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(kFloodCluster, 1, 1);
+        cfg.blockDim = dim3(kFloodThreads, 1, 1);
+        cfg.dynamicSmemBytes = band_bytes;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, flood_cluster_kernel, &cfg) == cudaSuccess && clusters > 0) {
+            flood_cluster_kernel<<<kFloodCluster, kFloodThreads, band_bytes, s>>>(m, o, height, width, wpr, hb);
+            fill_bits_kernel<<<blocks_for(n), 256, 0, s>>>(o, height, width, wpr, mask);
+            return cudaGetLastError() == cudaSuccess ? B200_OK : B200_ERUNTIME;
+        }
+        cudaGetLastError();
+    }
+    // else one CTA, the two planes in its shared memory when they fit (720p: 225 KB)
     const size_t planes = size_t(2) * height * wpr * 4;
     const bool in_smem = planes <= size_t(optin);
     if (in_smem && planes > 48 * 1024 &&
@@ -1198,6 +1227,9 @@ int b200_text_mask_device(const float *edge, const float *sd, int height, int wi
     fill_bits_kernel<<<blocks_for(n), 256, 0, s>>>(o, height, width, wpr, mask);
     return cudaGetLastError() == cudaSuccess ? B200_OK : B200_ERUNTIME;
 }
+
+// frames per group of coarse tracking's tables (two groups resident)
+constexpr int kCoarseGroup = 8;
 
 int b200_coarse_track_device(b200_handle *h, const uint8_t *frames, int n, int pitch, const uint8_t *keep,
                              double min_peak, int reset, int32_t *gross, double *prev, double *params, int32_t *used,
@@ -1255,20 +1287,21 @@ int b200_coarse_track_device(b200_handle *h, const uint8_t *frames, int n, int p
         const int64_t fstride = int64_t(pitch) * h->height;
         FitArgs fa{h->d_cpeaks.p, gross, keep, h->d_down.p, h->d_across.p, h->W / 2, h->ny, h->nx, h->height,
                    h->width, h->W, h->R, min_peak, prev, nullptr, nullptr};
-        // two sets of tables: those of group g + 1 are built on the side stream while the frames of
-        // group g are tracked on `stream` (the chain of one frame leaves most SMs idle)
+        // two sets of tables of up to kCoarseGroup frames: those of group g + 1 are built on the side
+        // stream while the frames of group g are tracked on `stream` (the chain of one frame leaves
+        // most SMs idle, and the tables of a group take a fraction of its chain)
+        const int G = std::min(h->group, kCoarseGroup);
         if (!h->d_csat.p) {
-            const size_t G = size_t(h->group);
-            h->d_csat.alloc(G * h->sat_size());
-            h->d_csat2.alloc(G * h->sat_size());
-            h->d_cdinv.alloc(G * h->dinv_size());
+            h->d_csat.alloc(2 * size_t(G) * h->sat_size());
+            h->d_csat2.alloc(2 * size_t(G) * h->sat_size());
+            h->d_cdinv.alloc(2 * size_t(G) * h->dinv_size());
         }
-        uint32_t *sat[2] = {h->d_sat.p, h->d_csat.p};
-        int64_t *sat2[2] = {h->d_sat2.p, h->d_csat2.p};
-        float *dinv[2] = {h->d_dinv.p, h->d_cdinv.p};
+        uint32_t *sat[2] = {h->d_csat.p, h->d_csat.p + size_t(G) * h->sat_size()};
+        int64_t *sat2[2] = {h->d_csat2.p, h->d_csat2.p + size_t(G) * h->sat_size()};
+        float *dinv[2] = {h->d_cdinv.p, h->d_cdinv.p + size_t(G) * h->dinv_size()};
         cudaEvent_t *ready = h->coarse_ev, *consumed = h->coarse_ev + 2, start = h->coarse_ev[4];
         cudaStream_t side = h->copy;
-        const int G = h->group, groups = (n + G - 1) / G;
+        const int groups = (n + G - 1) / G;
         auto tables = [&](int g) {
             const int nf = std::min(G, n - g * G);
             if (g >= 2) CK(cudaStreamWaitEvent(side, consumed[g % 2], 0));

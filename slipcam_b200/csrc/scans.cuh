@@ -7,6 +7,8 @@
 
 #include <cstdint>
 
+#include <cooperative_groups.h>
+
 #include "dft.cuh"
 
 namespace b200 {
@@ -16,7 +18,8 @@ constexpr int kSelectBins = 2048;     // bins of a pass of the percentile's radi
 constexpr int kSelectScratch = 256 + 2 * kSelectBins * 4;   // its state and two histograms, bytes
 constexpr int kDilateRows = 16;       // rows a CTA of the bit dilation writes
 constexpr int kDilateStep = 8;        // dilation steps per launch (the tile's halo rows)
-constexpr int kFloodThreads = 1024;   // the one CTA of the hole filling
+constexpr int kFloodThreads = 1024;   // threads per CTA of the hole filling
+constexpr int kFloodCluster = 8;      // CTAs of the clustered hole filling, a band of rows each
 
 #ifdef __CUDACC__
 
@@ -529,7 +532,7 @@ __device__ __forceinline__ bool vblock(const uint32_t *F, uint32_t *O, int h, in
         const bool in = q < nc && r < h && r >= 0;
         f[q] = in ? F[int64_t(r) * wpr + col[q]] : 0u;
         o[q] = in ? O[int64_t(r) * wpr + col[q]] : 0u;
-        A[q] = f[q];
+        A[q] = in ? f[q] : 0xFFFFFFFFu;   // rows past the end pass the carry through
         B[q] = o[q];
     }
 #pragma unroll
@@ -614,6 +617,132 @@ __global__ void __launch_bounds__(kFloodThreads, 1) flood_bits_kernel(uint32_t *
     }
     if (smem)
         for (int64_t i = threadIdx.x; i < words; i += blockDim.x) out[i] = O[i];
+}
+
+// the transfer of rows [0, rows) of column c of words (shared memory) in one direction: the
+// reached bits at the far end are B | A & (those entering at the near end); the blocks' warp scans
+// composed in order (identity: A = ~0, B = 0)
+__device__ __forceinline__ void vtransfer(const uint32_t *F, const uint32_t *O, int rows, int wpr, int c, bool down,
+                                          uint32_t &At, uint32_t &Bt)
+{
+    const int lane = threadIdx.x & 31, nb = (rows + 31) >> 5;
+    At = 0xFFFFFFFFu;
+    Bt = 0u;
+    for (int k = 0; k < nb; ++k) {
+        const int r = down ? 32 * k + lane : 32 * (nb - 1 - k) + 31 - lane;
+        uint32_t A = 0xFFFFFFFFu, B = 0u;
+        if (r < rows) {
+            A = F[int64_t(r) * wpr + c];
+            B = O[int64_t(r) * wpr + c];
+        }
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t a2 = __shfl_up_sync(0xffffffffu, A, d), b2 = __shfl_up_sync(0xffffffffu, B, d);
+            if (lane >= d) {
+                B |= A & b2;
+                A &= a2;
+            }
+        }
+        const uint32_t a = __shfl_sync(0xffffffffu, A, 31), b = __shfl_sync(0xffffffffu, B, 31);
+        Bt = b | (a & Bt);
+        At &= a;
+    }
+}
+
+// The hole filling by a cluster of kFloodCluster CTAs: CTA k holds rows [k hb, (k + 1) hb) of both
+// planes in its shared memory (`m`: the mask in global memory; `out`: the reached pixels). A sweep:
+// each CTA computes every column's transfer across its band, down and up, from its reached bits
+// as they stand; after a cluster barrier each composes the transfers of the bands above (down)
+// and below (up) into the carries entering its band, read from the other CTAs' shared memory, and
+// sweeps its band down and up with them; then its rows horizontally (hrow). The vertical result
+// equals the whole column's (a free run's pixels are reached when any pixel of the run is). The
+// sweeps end when no CTA changed a bit (an OR of per-CTA flags, two sets by sweep parity so a flag
+// is not rewritten before every CTA has read it); at most h * w + 1 sweeps, as the one-CTA form.
+// Every CTA takes the same barriers: the flags they OR are the same.
+__global__ void __cluster_dims__(kFloodCluster, 1, 1) __launch_bounds__(kFloodThreads, 1)
+    flood_cluster_kernel(const uint32_t *__restrict__ m, uint32_t *__restrict__ out, int h, int w, int wpr, int hb)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ uint32_t band[];
+    const int rank = int(cluster.block_rank()), lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int r0 = rank * hb, rows = max(0, min(h, r0 + hb) - r0);
+    const int64_t words = int64_t(hb) * wpr;
+    uint32_t *F = band, *O = band + words, *T = band + 2 * words;   // T: down A, down B, up A, up B (wpr each)
+    int *flag = reinterpret_cast<int *>(T + 4 * wpr);
+    for (int64_t i = threadIdx.x; i < int64_t(rows) * wpr; i += blockDim.x) {
+        const int lr = int(i / wpr), c = int(i - int64_t(lr) * wpr), r = r0 + lr;
+        const uint32_t f = ~m[int64_t(r) * wpr + c] & row_bits(c, w);
+        uint32_t edge = (c == 0 ? 1u : 0u) | (c == wpr - 1 ? 1u << ((w - 1) & 31) : 0u);
+        if (r == 0 || r == h - 1) edge = 0xFFFFFFFFu;
+        F[i] = f;
+        O[i] = f & edge;
+    }
+    __syncthreads();
+    bool go = true;
+    for (int64_t sweep = 0; go && sweep <= int64_t(h) * w; ++sweep) {
+        for (int c = warp; c < wpr; c += nwarp) {
+            uint32_t a, b;
+            vtransfer(F, O, rows, wpr, c, true, a, b);
+            if (lane == 0) {
+                T[c] = a;
+                T[wpr + c] = b;
+            }
+            vtransfer(F, O, rows, wpr, c, false, a, b);
+            if (lane == 0) {
+                T[2 * wpr + c] = a;
+                T[3 * wpr + c] = b;
+            }
+        }
+        cluster.sync();   // every band's transfers written
+        bool ch = false;
+        for (int c = warp; c < wpr; c += nwarp) {
+            // lane k < kFloodCluster reads band k's transfers; the carries compose them in order
+            uint32_t da = 0xFFFFFFFFu, db = 0u, ua = 0xFFFFFFFFu, ub = 0u;
+            if (lane < kFloodCluster && lane != rank) {
+                const uint32_t *t = cluster.map_shared_rank(T, lane);
+                da = t[c];
+                db = t[wpr + c];
+                ua = t[2 * wpr + c];
+                ub = t[3 * wpr + c];
+            }
+            uint32_t dc = 0u, uc = 0u;
+#pragma unroll
+            for (int k = 0; k < kFloodCluster; ++k) {
+                const uint32_t a = __shfl_sync(0xffffffffu, da, k), b = __shfl_sync(0xffffffffu, db, k);
+                if (k < rank) dc = b | (a & dc);
+            }
+#pragma unroll
+            for (int k = kFloodCluster - 1; k >= 0; --k) {
+                const uint32_t a = __shfl_sync(0xffffffffu, ua, k), b = __shfl_sync(0xffffffffu, ub, k);
+                if (k > rank) uc = b | (a & uc);
+            }
+            const int col[1] = {c};
+            uint32_t carry[1] = {dc};
+            for (int b0 = 0; b0 < rows; b0 += 32) ch |= vblock<1>(F, O, rows, wpr, col, 1, b0 + lane, carry);   // down
+            __syncwarp();
+            carry[0] = uc;
+            for (int b0 = ((rows - 1) >> 5) << 5; b0 >= 0; b0 -= 32) ch |= vblock<1>(F, O, rows, wpr, col, 1, b0 + 31 - lane, carry);
+            __syncwarp();
+        }
+        __syncthreads();
+        if (wpr <= 32)
+            ch |= hsweep<1>(F, O, rows, wpr);
+        else if (wpr <= 64)
+            ch |= hsweep<2>(F, O, rows, wpr);
+        else if (wpr <= 128)
+            ch |= hsweep<4>(F, O, rows, wpr);
+        else
+            ch |= hsweep<8>(F, O, rows, wpr);
+        const int any = __syncthreads_or(ch);
+        if (threadIdx.x == 0) flag[sweep & 1] = any;
+        cluster.sync();   // every CTA's flag written, every band's carries read
+        int all = 0;
+        if (threadIdx.x < kFloodCluster) all = *cluster.map_shared_rank(flag + (sweep & 1), int(threadIdx.x));
+        go = __syncthreads_or(all);
+    }
+    cluster.sync();   // no CTA leaves while another may still read its flags
+    for (int64_t i = threadIdx.x; i < int64_t(rows) * wpr; i += blockDim.x) out[int64_t(r0) * wpr + i] = O[i];
 }
 
 // the filled mask: every pixel the border's background does not reach
