@@ -1110,7 +1110,7 @@ int b200_chunk_std_median_device(const uint8_t *frames, int nchunks, int chunk, 
     if (smem > 48 * 1024 && cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
         return B200_ERUNTIME;
     const dim3 grid(unsigned((cols + kStdPixels - 1) / kStdPixels), unsigned(rows));
-    const dim3 block(32, unsigned(std::min(nchunks, kStdRegChunks)));
+    const dim3 block(32, unsigned(std::min(nchunks, 8)));   // 8 warps: four CTAs per SM, one's median beside another's loads
     if (narrow)
         chunk_std_median_kernel<uint32_t><<<grid, block, smem, static_cast<cudaStream_t>(stream)>>>(frames, fstride, step, rows,
                                                                                                   cols, chunk, nchunks, out);

@@ -100,4 +100,4 @@ def text_mask(frames, start, nframes=150, chunk=10, edge_percentile=90, max_std=
     scratch = torch.empty(_lib.lib().b200_text_mask_scratch_bytes(h, w), dtype=torch.uint8, device='cuda')
     _check(_lib.lib().b200_text_mask_device(edge.data_ptr(), sd.data_ptr(), h, w, float(edge_percentile), float(max_std),
                                             int(dilate), mask.data_ptr(), scratch.data_ptr(), scratch.numel(), stream))
-    return mask.cpu().numpy().astype(bool)
+    return mask.cpu().numpy().view(bool)   # the kernel writes 0 or 1
