@@ -1,8 +1,9 @@
 """
 Host frames to and from the device through pinned staging buffers. A pageable copy goes through the
 driver's own staging at about a fifth of the link's rate; here the copy between the caller's array
-and pinned memory is split over a pool of threads (numpy releases the GIL for it) and the DMA of one
-buffer overlaps the filling of the next. Used by the host-memory paths of scans and stabilize.
+and pinned memory is split over a pool of up to 8 threads (numpy releases the GIL for it; 16 ran
+slower beside the DMA) and the DMA of one buffer overlaps the filling of the next. Used by the
+host-memory paths of scans and stabilize.
 """
 
 import os
@@ -20,7 +21,7 @@ def _pool():
     global _POOL
     with _POOL_LOCK:
         if _POOL is None:
-            _POOL = ThreadPoolExecutor(max(1, min(8, os.cpu_count() or 1)), thread_name_prefix='framecor-stage')
+            _POOL = ThreadPoolExecutor(max(1, min(8, os.cpu_count() or 1)), thread_name_prefix="framecor-stage")
         return _POOL
 
 
