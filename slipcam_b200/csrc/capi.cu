@@ -1149,7 +1149,7 @@ int launch_percentile(const float *x, int64_t n, double q, float *out, void *scr
     auto *st = static_cast<SelectState *>(scratch);
     auto *hist = reinterpret_cast<uint32_t *>(static_cast<char *>(scratch) + 256);
     if (cudaMemsetAsync(scratch, 0, kSelectScratch, s) != cudaSuccess) return B200_ERUNTIME;
-    const unsigned grid = unsigned(std::clamp<int64_t>((n + 1023) / 1024, 1, 2 * sms));
+    const unsigned grid = unsigned(std::clamp<int64_t>((n + 4095) / 4096, 1, 2 * sms));   // 16 elements a thread or more
     for (int pass = 0; pass < 3; ++pass) select_pass_kernel<<<grid, 256, 0, s>>>(x, n, pass, lo, hi, t, st, hist, out);
     return cudaGetLastError() == cudaSuccess ? B200_OK : B200_ERUNTIME;
 }

@@ -269,8 +269,8 @@ __device__ __forceinline__ uint32_t cta_exclusive_sum_256(uint32_t x, uint32_t *
 
 // One pass of the selection of the statistics of ranks lo <= hi among x[0 .. n): pass 0 counts
 // the keys' bits 31..21, pass 1 bits 20..10 of the keys that share the picked top bits, pass 2
-// bits 9..0. A CTA counts in shared memory (the equal bins of a warp added once, by
-// __match_any_sync) and adds its counts to the histograms in global memory; the last CTA to finish
+// bits 9..0. A CTA counts in shared memory (four elements a thread per trip, their loads issued
+// together; the equal bins of a warp added once, by __match_any_sync) and adds its counts to the histograms in global memory; the last CTA to finish
 // (a ticket taken after a fence) picks each statistic's bin, narrows its rank, clears the
 // histograms for the next pass and, after pass 2, writes the percentile to *out: numpy's lerp in
 // float32, a + (b - a) * t for t < 0.5, else b - (b - a) * (1 - t), each step rounded.
@@ -289,18 +289,27 @@ __global__ void __launch_bounds__(256) select_pass_kernel(const float *__restric
     for (int i = threadIdx.x; i < 2 * B; i += blockDim.x) (&cnt[0][0])[i] = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t base = int64_t(blockIdx.x) * blockDim.x; base < n; base += stride) {   // the same trips for a warp
-        const int64_t i = base + threadIdx.x;
-        const bool ok = i < n;
-        const uint32_t k = ok ? order_key(__ldg(x + i)) : 0u;
-        const uint32_t d = (k >> shift) & uint32_t(bins - 1);
+    constexpr int U = 4;   // elements per thread per trip, their loads issued together
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x * U;
+    for (int64_t base = int64_t(blockIdx.x) * blockDim.x * U; base < n; base += stride) {   // the same trips for a warp
+        float v[U];
 #pragma unroll
-        for (int s = 0; s < 2; ++s) {
-            if (s == 1 && !two) break;
-            const bool in = ok && (k & known) == (s ? p1 : p0);
-            const unsigned peers = __match_any_sync(0xffffffffu, in ? d : 0xFFFFFFFFu);
-            if (in && lane == __ffs(peers) - 1) atomicAdd(&cnt[s][d], unsigned(__popc(peers)));
+        for (int u = 0; u < U; ++u) {
+            const int64_t i = base + int64_t(u) * blockDim.x + threadIdx.x;
+            v[u] = i < n ? __ldg(x + i) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const bool ok = base + int64_t(u) * blockDim.x + threadIdx.x < n;
+            const uint32_t k = ok ? order_key(v[u]) : 0u;
+            const uint32_t d = (k >> shift) & uint32_t(bins - 1);
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                if (s == 1 && !two) break;
+                const bool in = ok && (k & known) == (s ? p1 : p0);
+                const unsigned peers = __match_any_sync(0xffffffffu, in ? d : 0xFFFFFFFFu);
+                if (in && lane == __ffs(peers) - 1) atomicAdd(&cnt[s][d], unsigned(__popc(peers)));
+            }
         }
     }
     __syncthreads();
