@@ -271,7 +271,7 @@ def run_b200(args):
     value = world * args.steps * BATCH * nwin / (ms / 1e3)
 
     # the other form on the same steps (device time), for comparison
-    other = 'fft32' if args.form == 'tc' else 'tc'
+    other = 'fft32' if args.form in ('tc', 'int8') else 'tc'
     cor.set_form(other)
     for i in range(2):
         step_dev(i)
@@ -285,7 +285,8 @@ def run_b200(args):
     cor.set_form(args.form)
 
     if args.no_e2e:
-        print(json.dumps({'value': value, 'kernel_ms': kernel_ms, 'kernel_launches': kernel_launches}))
+        print(json.dumps({'value': value, 'form': args.form, 'kernel_ms': kernel_ms, 'kernel_launches': kernel_launches,
+                          'other_form': other, 'other_value': other_value, 'clocks': clk}))
         return
     # end to end through the host entry point: frames in page-locked memory, numpy outputs
     host = torch.empty(frames.shape, dtype=torch.uint8, pin_memory=True)
@@ -752,7 +753,7 @@ def main():
     p.add_argument('--no-e2e', action='store_true', help='device timing only (profiling runs)')
     p.add_argument('--video', type=int, default=NFRAMES, help='frames of the synthetic video to render')
     p.add_argument('--batch', type=int, default=BATCH, help='frames per step')
-    p.add_argument('--form', default='tc', choices=['fft32', 'tc'], help='the arithmetic of the transforms')
+    p.add_argument('--form', default='tc', choices=['fft32', 'tc', 'int8'], help='the arithmetic of the transforms')
     p.add_argument('--workload', default='hd', choices=['hd', 'mixed', 'stream', 'diff', 'stabilize', 'scans'],
                    help='hd: the 720p headline; mixed: three grids in one group step; stream: 1080p streaming; '
                         'diff: the differentiable path; stabilize: coarse similarity tracking; '

@@ -53,6 +53,9 @@ extern "C" {
 #define B200_FORM_AUTO 0   /* the library's choice */
 #define B200_FORM_FFT32 1  /* FP32 FFTs on the CUDA cores */
 #define B200_FORM_TC 2     /* DFT-matrix GEMMs on the tensor cores, FP16 operands, FP32 accumulation */
+#define B200_FORM_I8 3     /* direct correlation on the tensor cores in exact integers (uint8 x uint8,
+                              int32 accumulation), normalized after: windows up to 181 px, search
+                              windows (window + 2 search) up to 256 px */
 
 /* The frames, the grid of reference windows and the correlation parameters.
  * Replaces framecor::Params (cxx/framecor.h:22-35); same fields, same defaults in the binding
@@ -319,6 +322,15 @@ B200_API int b200_sat_device(const uint8_t *frames, int n, int height, int width
  * 256. Synchronous. B200_ETIMEOUT if the MMA completion wait gave up. No reference counterpart. */
 B200_API int b200_tc_selftest(const void *A, const void *B, float *D, int N, int K, int a_mn, int b_mn,
                               int neg_b, void *stream);
+
+/* A check of the exact form's tensor-core path: D (128 x N, int32) = A (128 x K) x X[i .. i + N - 1]^T,
+ * uint8 row-major device arrays (X has `rows` rows), computed by one CTA with tcgen05.mma kind::i8:
+ * A written to tensor memory (or, a_smem != 0, staged in shared memory), X staged in shared memory as
+ * the exact form holds a search window (the operand started at row i). N a multiple of 16 up to 256,
+ * K a multiple of 32 up to 256. Synchronous. B200_ETIMEOUT if the MMA completion wait gave up. No
+ * reference counterpart. */
+B200_API int b200_tc_i8_selftest(const uint8_t *A, const uint8_t *X, int32_t *D, int N, int K, int rows, int i,
+                                 int a_smem, void *stream);
 
 /* The arithmetic of the transforms, B200_FORM_*; B200_EINVAL for an unknown or unbuilt form. */
 B200_API int b200_set_form(b200_handle *h, int form);

@@ -11,7 +11,7 @@ LIB_PATH = os.path.join(HERE, 'libslipcam_b200.so')
 
 OK, EINVAL, ERUNTIME, ETIMEOUT = 0, 1, 2, 3
 GROSS_NONE, GROSS_FRAME, GROSS_WINDOW = 0, 1, 2
-FORM_AUTO, FORM_FFT32, FORM_TC = 0, 1, 2
+FORM_AUTO, FORM_FFT32, FORM_TC, FORM_I8 = 0, 1, 2, 3
 COARSE_MAX_WINDOWS = 2048
 PERCENTILE_SCRATCH = 16640   # bytes of device scratch of b200_percentile_f32_device
 
@@ -71,6 +71,7 @@ SIGNATURES = {
     'b200_sat_device': (_i, [_u8p, _i, _i, _i, _i, _vp, _vp, _vp]),
     'b200_set_form': (_i, [_vp, _i]),
     'b200_tc_selftest': (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _vp]),
+    'b200_tc_i8_selftest': (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _vp]),
     'b200_info': (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i),
                        ctypes.POINTER(ctypes.c_uint64)]),
     'b200_profile': (_i, [_vp, _i]),

@@ -23,6 +23,7 @@
 #include "corr_fft.cuh"
 #include "corr_big.cuh"
 #include "corr_tc.cuh"
+#include "corr_i8.cuh"
 #include "diff.h"
 #include "multi.h"
 #include "periodicity.cuh"
@@ -100,6 +101,7 @@ struct Slot {
     DevBuf<uint32_t> sat;
     DevBuf<int64_t> sat2;
     DevBuf<float> dinv;
+    DevBuf<int2> bstat;         // {box sum, dinv} beside dinv (the exact tensor-core form)
     DevBuf<int32_t> gross;
     DevBuf<float> out;          // offset 2P | peak P | snr P | cov 3P, P = group * nwin
     HostBuf<uint8_t> hframes;
@@ -251,6 +253,27 @@ void launch_corr_tc(const CorrArgs &a, const uint4 *dtab, int *status, const CUt
     corr_tc_kernel<N><<<unsigned(grid), kTcThreads, TcGeo<N>::smem_bytes, s>>>(a, dtab, status, dmap);
 }
 
+// the exact tensor-core form: one persistent CTA per SM over the groups of F frames of a window
+void launch_corr_i8(const CorrArgs &a, const uint8_t *refwin, const int *sref, int *status, const I8Geo &g, cudaStream_t s)
+{
+    static bool done[64] = {};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        CK(cudaFuncSetAttribute(corr_i8_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kI8MaxSmem)));
+        CK(cudaFuncSetAttribute(corr_i8_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kI8MaxSmem)));
+        done[dev] = true;
+    }
+    if (!a.bstat || !refwin || !sref) fail(B200_EINVAL, "the exact tensor-core form has no box table or reference windows");
+    const int groups = a.nwin * ((a.nf + g.F - 1) / g.F);
+    const int grid = std::min(groups, num_sms());
+    const I8Args x{a, a.bstat, refwin, sref, status, g};
+    if (a.surface)
+        corr_i8_kernel<true><<<unsigned(grid), kI8Threads, g.smem, s>>>(x);
+    else
+        corr_i8_kernel<false><<<unsigned(grid), kI8Threads, g.smem, s>>>(x);
+}
+
 template <int N>
 bool tc_fits_n(int M)
 {
@@ -334,6 +357,7 @@ struct b200_handle {
     int group = 1;
     int form = B200_FORM_FFT32;
     bool ready = false;
+    bool ref_u8 = false;         // the reference is a uint8 frame (the exact form's windows are set)
     uint64_t launches = 0;
     std::string err;
     cudaStream_t comp = nullptr, copy = nullptr;
@@ -343,6 +367,9 @@ struct b200_handle {
     DevBuf<float4> d_spec_tc;    // the reference spectra in the tensor-core form's order
     DevBuf<float2> d_big;        // the big transform's per-CTA scratch (N = 256 only)
     DevBuf<uint8_t> d_ref;
+    DevBuf<uint8_t> d_refwin;    // the exact tensor-core form: the reference windows' pixels, nwin x W x W
+    DevBuf<int> d_sref;          // and their sums
+    DevBuf<int2> d_bstat;        // device-path box table (beside d_dinv)
     DevBuf<uint32_t> d_sat;      // device-path scratch
     DevBuf<int64_t> d_sat2;
     DevBuf<float> d_dinv;
@@ -359,6 +386,8 @@ struct b200_handle {
     cudaEvent_t coarse_ev[6] = {};  // coarse tracking: tables ready (2), tables consumed (2), call start, end
     bool coarse_l2 = false;      // the handle's stream keeps the reference spectra in L2
     bool tc_ok = false;          // the geometry fits the tensor-core kernel
+    bool i8_ok = false;          // the geometry fits the exact tensor-core kernel
+    I8Geo i8g{};                 // its layout
     int fpitch = 0;              // the pitch of the staged frames (a multiple of 16)
     bool profiling = false;      // events around the correlation launches
     struct Timed {
@@ -395,6 +424,7 @@ struct b200_handle {
             s.sat.alloc(G * sat_size());
             s.sat2.alloc(G * sat_size());
             s.dinv.alloc(G * dinv_size());
+            if (i8_ok) s.bstat.alloc(G * dinv_size());
             s.gross.alloc(2 * P);
             s.out.alloc(7 * P);
             s.hframes.alloc(G * height * fpitch);
@@ -420,29 +450,35 @@ struct b200_handle {
         d_sat.alloc(G * sat_size());
         d_sat2.alloc(G * sat_size());
         d_dinv.alloc(G * dinv_size());
+        if (i8_ok) d_bstat.alloc(G * dinv_size());
         if (tc_ok) {
             const CUtensorMap m = dinv_map(d_dinv.p, height, width, dpitch(), int(G), M);
             CK(cudaMemcpy(d_tmaps.p + 2, &m, sizeof(m), cudaMemcpyHostToDevice));
         }
     }
 
-    // the tables and the correlation of nf frames (device memory) on stream s
+    // the tables and the correlation of nf frames (device memory) on stream s; bstat (the box table
+    // beside dinv) serves the exact tensor-core form
     void run_group(const uint8_t *frames, int pitch, int nf, const int32_t *gross, int gross_mode,
-                   uint32_t *sat, int64_t *sat2, float *dinv, float *offset, float *peak, float *snr,
+                   uint32_t *sat, int64_t *sat2, float *dinv, int2 *bstat, float *offset, float *peak, float *snr,
                    float *cov, float *surface, cudaStream_t s)
     {
-        run_tables(frames, pitch, nf, sat, sat2, dinv, s);
-        run_corr(frames, pitch, nf, gross, gross_mode, sat, dinv, offset, peak, snr, cov, surface, form, s);
+        const int arith = form != B200_FORM_I8 ? form : (bstat && ref_u8) ? B200_FORM_I8 : B200_FORM_FFT32;
+        run_tables(frames, pitch, nf, sat, sat2, dinv, s, arith == B200_FORM_I8 ? bstat : nullptr);
+        CorrArgs a = corr_args(frames, pitch, nf, gross, gross_mode, sat, dinv, offset, peak, snr, cov, surface);
+        a.bstat = bstat;
+        run_corr_tail(a, nf, dinv, arith, s);
         launches += 3;
     }
 
-    // the summed-area tables and the variance denominators of nf frames
-    void run_tables(const uint8_t *frames, int pitch, int nf, uint32_t *sat, int64_t *sat2, float *dinv, cudaStream_t s)
+    // the summed-area tables and the variance denominators of nf frames (and the box table)
+    void run_tables(const uint8_t *frames, int pitch, int nf, uint32_t *sat, int64_t *sat2, float *dinv, cudaStream_t s,
+                    int2 *bstat = nullptr)
     {
         const int64_t fstride = int64_t(pitch) * height;
         launch_sat(frames, fstride, pitch, nf, height, width, sat, sat2, s);
         dinv_kernel<<<dim3(unsigned((width - W + 1 + 127) / 128), unsigned(height - W + 1), unsigned(nf)), 128, 0, s>>>(
-            sat, sat2, sat_size(), height, width, W, dinv, dinv_size(), dpitch());
+            sat, sat2, sat_size(), height, width, W, dinv, dinv_size(), dpitch(), bstat);
     }
 
     // the correlation of nf frames with their tables at sat / dinv, in the form `arith`
@@ -504,7 +540,9 @@ struct b200_handle {
             t.pairs = uint64_t(nf) * nwin;
             CK(cudaEventRecord(t.a, s));
         }
-        if (arith == B200_FORM_TC) {
+        if (arith == B200_FORM_I8) {
+            launch_corr_i8(a, d_refwin.p, d_sref.p, d_status.p, i8g, s);
+        } else if (arith == B200_FORM_TC) {
             const uint4 *dt = reinterpret_cast<const uint4 *>(d_dtab.p);
             const int mi = dinv == slot[0].dinv.p ? 0 : dinv == slot[1].dinv.p ? 1 : 2;
             if (mi == 2 && dinv != d_dinv.p) fail(B200_EINVAL, "no TMA map for this denominator table");
@@ -611,6 +649,13 @@ void upload_reference(b200_handle *h, const uint8_t *dframe, int pitch, cudaStre
     h->launches += 1;
     if (h->tc_ok) {
         spec_tc_kernel<<<unsigned(4 * num_sms()), 256, 0, s>>>(h->d_spec.p, h->d_spec_tc.p, h->N, h->nwin);
+        CK(cudaGetLastError());
+        h->launches += 1;
+    }
+    h->ref_u8 = !dframef;
+    if (h->i8_ok && !dframef) {
+        refwin_kernel<<<unsigned(h->nwin), 128, 0, s>>>(dframe, pitch, h->W, h->nx, h->d_down.p, h->d_across.p,
+                                                          h->d_refwin.p, h->d_sref.p);
         CK(cudaGetLastError());
         h->launches += 1;
     }
@@ -729,6 +774,11 @@ int b200_create(const b200_params *p, int device, b200_handle **out)
             CK(cudaMemcpy(h->d_dtab.p, dt.data(), dt.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
         }
         if (N == kBigN) h->d_big.alloc(size_t(num_sms()) * big_scratch_per_cta(L, h->M));
+        h->i8_ok = i8_plan(h->W, h->R, h->i8g);
+        if (h->i8_ok) {
+            h->d_refwin.alloc(size_t(h->nwin) * h->W * h->W);
+            h->d_sref.alloc(h->nwin);
+        }
         // the maps of the two slots and of the device path's table are written when those are allocated
         if (h->tc_ok) h->d_tmaps.alloc(3);
         *out = h;
@@ -760,11 +810,15 @@ const char *b200_last_error(const b200_handle *h) { return h ? h->err.c_str() : 
 int b200_set_form(b200_handle *h, int form)
 {
     return guarded(h, [&] {
-        if (form != B200_FORM_AUTO && form != B200_FORM_FFT32 && form != B200_FORM_TC)
+        if (form != B200_FORM_AUTO && form != B200_FORM_FFT32 && form != B200_FORM_TC && form != B200_FORM_I8)
             fail(B200_EINVAL, "unknown form " + std::to_string(form));
         if (form == B200_FORM_TC && !h->tc_ok)
             fail(B200_EINVAL, "the tensor-core form holds FFT sizes up to 160 and search ranges up to 63 px, not "
                                   + std::to_string(h->N) + " and " + std::to_string(h->R));
+        if (form == B200_FORM_I8 && !h->i8_ok)
+            fail(B200_EINVAL, "the exact tensor-core form holds windows up to " + std::to_string(kI8MaxWindow)
+                                  + " px and search windows up to 256 px, not " + std::to_string(h->W) + " and "
+                                  + std::to_string(h->L));
         h->form = form == B200_FORM_AUTO ? B200_FORM_FFT32 : form;
     });
 }
@@ -848,7 +902,7 @@ int b200_correlate(b200_handle *h, const uint8_t *frames, int n, const int32_t *
             CK(cudaEventRecord(s.in, h->copy));
             CK(cudaStreamWaitEvent(h->comp, s.in, 0));
             float *o = s.out.p;
-            h->run_group(s.frames.p, h->fpitch, nf, dg, gross_mode, s.sat.p, s.sat2.p, s.dinv.p, o, o + 2 * PG,
+            h->run_group(s.frames.p, h->fpitch, nf, dg, gross_mode, s.sat.p, s.sat2.p, s.dinv.p, s.bstat.p, o, o + 2 * PG,
                          o + 3 * PG, o + 4 * PG, nullptr, h->comp);
             CK(cudaMemcpyAsync(s.hout.p, s.out.p, 7 * PG * sizeof(float), cudaMemcpyDeviceToHost, h->comp));
             CK(cudaEventRecord(s.done, h->comp));
@@ -885,7 +939,7 @@ static int correlate_device(b200_handle *h, const uint8_t *frames, int n, int pi
             const size_t q0 = size_t(f0) * nwin;
             const int32_t *g = gross_mode == B200_GROSS_FRAME ? gross + 2 * size_t(f0)
                              : gross_mode == B200_GROSS_WINDOW ? gross + 2 * q0 : nullptr;
-            h->run_group(frames + f0 * fstride, pitch, nf, g, gross_mode, h->d_sat.p, h->d_sat2.p, h->d_dinv.p,
+            h->run_group(frames + f0 * fstride, pitch, nf, g, gross_mode, h->d_sat.p, h->d_sat2.p, h->d_dinv.p, h->d_bstat.p,
                          offset + 2 * q0, peak + q0, snr + q0, cov + 3 * q0,
                          surface ? surface + q0 * size_t(h->M) * h->M : nullptr, s);
         }
@@ -1042,6 +1096,29 @@ int b200_tc_selftest(const void *A, const void *B, float *D, int N, int K, int a
     if (cudaFuncSetAttribute(tc_selftest_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
         return B200_ERUNTIME;
     tc_selftest_kernel<<<1, 128, smem, s>>>(a);
+    int h = 0;
+    const bool ok = cudaGetLastError() == cudaSuccess && cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, s) == cudaSuccess
+                    && cudaStreamSynchronize(s) == cudaSuccess;
+    cudaFreeAsync(status, s);
+    if (!ok) return B200_ERUNTIME;
+    return h ? B200_ETIMEOUT : B200_OK;
+}
+
+int b200_tc_i8_selftest(const uint8_t *A, const uint8_t *X, int32_t *D, int N, int K, int rows, int i, int a_smem,
+                        void *stream)
+{
+    if (!A || !X || !D || N < 16 || N > 256 || N % 16 || K < 32 || K % 32 || K > 256 || i < 0 || rows < i + N
+        || size_t(rows | 1) * K + 128 * size_t(K) > 200 * 1024)
+        return B200_EINVAL;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int *status = nullptr;
+    if (cudaMallocAsync(&status, sizeof(int), s) != cudaSuccess) return B200_ERUNTIME;
+    cudaMemsetAsync(status, 0, sizeof(int), s);
+    const I8SelftestArgs a{A, X, D, N, K, rows, i, a_smem, status};
+    const size_t smem = ((size_t(rows | 1) * K + 127) & ~size_t(127)) + 128 * size_t(K);
+    if (cudaFuncSetAttribute(tc_i8_selftest_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+        return B200_ERUNTIME;
+    tc_i8_selftest_kernel<<<1, 128, smem, s>>>(a);
     int h = 0;
     const bool ok = cudaGetLastError() == cudaSuccess && cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, s) == cudaSuccess
                     && cudaStreamSynchronize(s) == cudaSuccess;

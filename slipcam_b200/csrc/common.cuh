@@ -65,6 +65,8 @@ struct CorrArgs {
     float *surface;            // nullptr, or nf x nwin x M x M: the normalized surfaces
     double *ncc;               // nullptr, or nf x nwin x 3: stabilize.ncc_peak's (dy, dx, value) of each
                                // surface ((NaN, NaN, -inf) for an invalid pair)
+    const int2 *bstat;         // nullptr, or nf x h x dpitch: {pixel sum, dinv bits} of each W x W box
+                               // (the exact tensor-core form's table, beside dinv)
 };
 
 }   // namespace b200

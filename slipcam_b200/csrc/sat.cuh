@@ -120,9 +120,11 @@ __global__ void __launch_bounds__(256) sat_cols_kernel(int h, int w, uint32_t *s
         }
 }
 
-// dinv[y][x] (row pitch dpitch floats) for the W x W boxes at (y, x), y <= h - W, x <= w - W
+// dinv[y][x] (row pitch dpitch floats) for the W x W boxes at (y, x), y <= h - W, x <= w - W; and,
+// when bstat is given, {the box's pixel sum, the bits of its dinv} in the same layout
 __global__ void __launch_bounds__(128) dinv_kernel(const uint32_t *sat, const int64_t *sat2, int64_t sfs,
-                                                   int h, int w, int W, float *dinv, int64_t dfs, int dpitch)
+                                                   int h, int w, int W, float *dinv, int64_t dfs, int dpitch,
+                                                   int2 *bstat = nullptr)
 {
     const int x = blockIdx.x * 128 + threadIdx.x, y = blockIdx.y, f = blockIdx.z;
     if (x > w - W || y > h - W) return;
@@ -134,7 +136,9 @@ __global__ void __launch_bounds__(128) dinv_kernel(const uint32_t *sat, const in
     const int64_t bs2 = s2[d] - s2[b] - s2[c] + s2[a];
     const int64_t n = int64_t(W) * W;
     const int64_t v = n * bs2 - bs * bs;
-    dinv[f * dfs + size_t(y) * dpitch + x] = v > 0 ? float(1.0 / sqrt(double(v) / double(n))) : 0.0f;
+    const float di = v > 0 ? float(1.0 / sqrt(double(v) / double(n))) : 0.0f;
+    dinv[f * dfs + size_t(y) * dpitch + x] = di;
+    if (bstat) bstat[f * dfs + size_t(y) * dpitch + x] = make_int2(int(bs), __float_as_int(di));
 }
 
 #endif   // __CUDACC__

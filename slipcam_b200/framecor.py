@@ -124,8 +124,10 @@ class Correlator:
 
     def set_form(self, form):
         """The arithmetic of the transforms: 'fft32' (FP32 FFTs on the CUDA cores), 'tc' (DFT-matrix
-        GEMMs on the tensor cores, FP16 operands, FP32 accumulation) or 'auto'."""
-        code = {'auto': _lib.FORM_AUTO, 'fft32': _lib.FORM_FFT32, 'tc': _lib.FORM_TC}.get(form)
+        GEMMs on the tensor cores, FP16 operands, FP32 accumulation), 'int8' (the correlation summed
+        directly on the tensor cores in exact integers, then normalized) or 'auto'."""
+        code = {'auto': _lib.FORM_AUTO, 'fft32': _lib.FORM_FFT32, 'tc': _lib.FORM_TC,
+                'int8': _lib.FORM_I8}.get(form)
         if code is None:
             raise ValueError(f'framecor: unknown form {form}')
         _lib.raise_for(_lib.lib().b200_set_form(self._h, code), self._h)

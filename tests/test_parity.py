@@ -24,9 +24,6 @@ torch = pytest.importorskip('torch')
 
 SUPPORTED = list(cases.NAMES)   # 'big' (window 128 + search 64, L = 256) runs the staged big transform
 NEAR_TIE = 1e-5
-# the share of integer peaks allowed to differ, each one a verified near-tie; 'mixed' has periodic
-# stripes (8 px) whose surfaces have exactly equal maxima, decided by rounding alone
-TIE_SHARE = {'mixed': 0.2}
 
 
 def golden(name):
@@ -40,23 +37,29 @@ def b200(c, gross=None, frames=None):
     return cor, cor.correlate(c['frames'] if frames is None else frames, gross=c['gross'] if gross is None else gross)
 
 
-def near_tie_ok(c, mism, out, ref_out, tol):
+def sub(c, sl):
+    """The windows and the gross offsets of the sub-grid sl (frames, rows, columns) of case c."""
+    g = oracle.expand_gross(c['gross'], len(c['frames']), len(c['down']), len(c['across']))
+    return c['down'][sl[1]], c['across'][sl[2]], None if g is None else g[sl]
+
+
+def fp64_surface(c, down, across, gross, f, y, x):
+    g = None if gross is None else gross[f:f + 1, y:y + 1, x:x + 1]
+    o = oracle.correlate(c['height'], c['width'], down[y:y + 1], across[x:x + 1], c['reference'],
+                         c['frames'][f:f + 1], g, window=c['window'], search=c['search'],
+                         stat_size=c['stat_size'], mode='f64', surfaces=True)
+    return o['surface'][0, 0, 0], (0, 0) if g is None else tuple(g[0, 0, 0])
+
+
+def near_tie_ok(c, mism, out, ref_out, tol, sl=(slice(None),) * 3):
     """Mismatched integer peaks are near-ties: on the oracle's FP64 surface the value at each
-    side's peak shift is within tol of the maximum."""
+    side's peak shift is within tol of the maximum (out and ref_out on the sub-grid sl)."""
     if not mism.any():
         return True
-    idx = np.argwhere(mism)
-    f, y, x = idx[:, 0], idx[:, 1], idx[:, 2]
-    ny, nx = len(c['down']), len(c['across'])
-    g = oracle.expand_gross(c['gross'], len(c['frames']), ny, nx)
+    down, across, gross = sub(c, sl)
     R, M = c['search'], 2 * c['search'] + 1
-    for ff, yy, xx in zip(f, y, x):
-        gross = None if g is None else g[ff:ff + 1, yy:yy + 1, xx:xx + 1]
-        o = oracle.correlate(c['height'], c['width'], c['down'][yy:yy + 1], c['across'][xx:xx + 1], c['reference'],
-                             c['frames'][ff:ff + 1], gross, window=c['window'], search=R,
-                             stat_size=c['stat_size'], mode='f64', surfaces=True)
-        s = o['surface'][0, 0, 0]
-        gy, gx = (0, 0) if gross is None else gross[0, 0, 0]
+    for ff, yy, xx in np.argwhere(mism):
+        s, (gy, gx) = fp64_surface(c, down, across, gross, ff, yy, xx)
         for res in (out, ref_out):
             u = int(np.rint(res['offsets'][ff, yy, xx, 0] - gy + R))
             v = int(np.rint(res['offsets'][ff, yy, xx, 1] - gx + R))
@@ -64,6 +67,27 @@ def near_tie_ok(c, mism, out, ref_out, tol):
             if s.max() - cand > tol:
                 return False
     return True
+
+
+def tie_count(c, tol=NEAR_TIE, sl=(slice(None),) * 3):
+    """The pairs whose FP64 surface holds a second integer peak, outside the maximum's 3 x 3, within
+    tol of the maximum: the only pairs whose integer peak rounding may decide. 'mixed' (flat,
+    saturated and 8 px striped regions) has 182 such pairs of 456, all exact ties; the other cases
+    have none."""
+    down, across, gross = sub(c, sl)
+    o = oracle.correlate(c['height'], c['width'], down, across, c['reference'], c['frames'], gross,
+                         window=c['window'], search=c['search'], stat_size=c['stat_size'], mode='f64', surfaces=True)
+    M = 2 * c['search'] + 1
+    flat = o['surface'].reshape(-1, M * M)
+    valid = np.isfinite(o['offsets'][..., 0]).reshape(-1)
+    n = 0
+    for p in np.flatnonzero(valid):
+        f = flat[p]
+        u, v = divmod(int(np.argmax(f)), M)
+        g = f.reshape(M, M).copy()
+        g[max(u - 1, 0):u + 2, max(v - 1, 0):v + 2] = -np.inf
+        n += int(f.max() - g.max() <= tol)
+    return n
 
 
 @pytest.mark.parametrize('name', SUPPORTED)
@@ -79,8 +103,9 @@ def test_golden(name):
     assert np.all(r['cov'][~valid] == np.array([99, 99, 0], np.float32))
     d = np.abs(a - b).max(-1)
     mism = valid & (d > 0.5)
-    assert mism.sum() <= max(1, int(valid.sum() * TIE_SHARE.get(name, 0.01))), f'{mism.sum()} integer peaks differ'
-    assert near_tie_ok(c, mism, r, g, NEAR_TIE)
+    if mism.any():   # every differing integer peak is a verified near-tie, and there are no more than ties
+        assert mism.sum() <= tie_count(c), f'{mism.sum()} integer peaks differ'
+        assert near_tie_ok(c, mism, r, g, NEAR_TIE)
     ok = valid & ~mism
     assert d[ok].max() < 1e-3, d[ok].max()
     assert np.abs(g['peak'][ok] - r['peak'][ok]).max() < 1e-4
@@ -104,8 +129,9 @@ def test_fp64_oracle(name):
     valid = np.isfinite(o['offsets'][..., 0])
     d = np.abs(o['offsets64'] - b['offsets']).max(-1)
     mism = valid & (d > 0.5)
-    assert mism.sum() <= max(1, int(valid.sum() * TIE_SHARE.get(name, 0.01)))
-    assert near_tie_ok(c, mism, b, o, NEAR_TIE) if gross is None or gross.ndim == 2 else True
+    if mism.any():   # per-frame and per-window gross alike
+        assert mism.sum() <= tie_count(c, sl=sl)
+        assert near_tie_ok(c, mism, b, o, NEAR_TIE, sl)
     ok = valid & ~mism
     assert d[ok].max() < 0.01, d[ok].max()
     assert np.abs(b['snr'][ok] / o['snr'][ok] - 1).max() < 1e-3
@@ -199,6 +225,7 @@ def test_hd_recovers_motion():
 # clean, sharp peaks (small patch sums): there the typical error stays below 2e-3 px and at most 5 %
 # of the pairs (2 in a small case) may exceed 0.01 px, none by more than 0.1 px.
 TC_CASES = ['shifts', 'gross', 'window_gross', 'invalid', 'small', 'hd', 'mixed']
+TC_NEAR_TIE = 2e-3   # a near-tie for the FP16 form: within a few times its surface error (3e-4)
 
 
 @pytest.mark.parametrize('name', TC_CASES)
@@ -222,7 +249,9 @@ def test_tc_fp64_oracle(name):
     assert np.all(b['cov'][~valid] == np.array([99, 99, 0], np.float32))
     d = np.abs(o['offsets64'] - b['offsets']).max(-1)
     mism = valid & (d > 0.5)
-    assert mism.sum() <= max(1, int(valid.sum() * TIE_SHARE.get(name, 0.01)))
+    if mism.any():   # each one a near-tie within the FP16 surface error
+        assert mism.sum() <= tie_count(c, TC_NEAR_TIE, sl)
+        assert near_tie_ok(c, mism, b, o, TC_NEAR_TIE, sl)
     ok = valid & ~mism
     assert np.abs(b['peak'][ok] - o['peak'][ok]).max() < 1e-3
     snr_rel = np.abs(b['snr'][ok] / o['snr'][ok] - 1)
