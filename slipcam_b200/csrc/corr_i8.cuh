@@ -36,13 +36,14 @@
 
 #include <algorithm>
 #include <climits>
+#include <type_traits>
 
 #include "corr_fft.cuh"
 #include "tc.cuh"
 
 namespace b200 {
 
-constexpr int kI8Producers = 4;
+constexpr int kI8Producers = 8;   // two per TMEM lane quadrant, taking alternate ring stages
 constexpr int kI8Epilogue = 4;
 constexpr int kI8Threads = 32 * (kI8Producers + kI8Epilogue + 1);
 constexpr int kI8Mma = 32 * (kI8Producers + kI8Epilogue);   // the thread that issues the MMAs
@@ -203,8 +204,7 @@ __device__ __forceinline__ void mma(uint32_t d_tmem, uint32_t a_tmem, uint64_t b
 __device__ __forceinline__ void st8(uint32_t taddr, const uint32_t (&w)[8])
 {
     asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr), "r"(w[0]),
-                 "r"(w[1]), "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7])
-                 : "memory");
+                 "r"(w[1]), "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7]));
 }
 __device__ __forceinline__ void st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) corr_i8_kernel(I8Args args)
     if (warp == 0) tc::tmem_alloc(&tmem_base, 512);
     if (tid == 0) {
         for (int s = 0; s < NS; ++s) {
-            tc::mbar_init(&bar_full[s], kI8Producers);
+            tc::mbar_init(&bar_full[s], 4);   // the four producer warps (one per quadrant) of the stage
             tc::mbar_init(&bar_empty[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
@@ -294,10 +294,10 @@ __global__ void __launch_bounds__(kI8Threads, 1) corr_i8_kernel(I8Args args)
         // ---- producers: the Toeplitz chunks of each reference row, one ring stage per row. No early
         // exit: the named barrier below must see all four warps, so after a failed wait a warp keeps
         // walking the groups without work (every wait returns at once once aborted).
-        const int qd = warp;
+        const int qd = warp & 3, half = warp >> 2;   // lane quadrant; the stages of this warp: parity half
         const uint32_t lane_addr = tmem + (uint32_t(32 * qd) << 16) + g.ring_col;
         int s = 0;
-        uint32_t round = 0;
+        uint32_t round = 0, seq = 0;   // ring position; stages filled so far by the CTA (both halves)
         int cur_k = -1;
         for (int gl = 0;; ++gl) {
             const int gi = blockIdx.x + gl * gridDim.x;
@@ -313,30 +313,33 @@ __global__ void __launch_bounds__(kI8Threads, 1) corr_i8_kernel(I8Args args)
                 asm volatile("bar.sync 1, %0;" ::"n"(32 * kI8Producers) : "memory");
                 cur_k = k;
             }
-            for (int i = 0; i < W; ++i) {
-                if (!*abort && (round == 0 || i8::wait(&bar_empty[s], (round - 1) & 1u, abort))) {
+            for (int i = 0; i < W; ++i, ++seq) {
+                if ((seq & 1u) == uint32_t(half) && !*abort && (round == 0 || i8::wait(&bar_empty[s], (round - 1) & 1u, abort))) {
                     tc::fence_after_sync();
                     const uint32_t *row = reinterpret_cast<const uint32_t *>(P + i * g.pw);
                     uint32_t col = lane_addr + uint32_t(s) * g.stage_cols;
                     for (int vt = 0; vt < VT; ++vt) {
-                        // bytes 128 + 32 c - v .. of the padded row: T_i[v][32 c ..] = ref(i, 32 c - v ..)
+                        // bytes 128 + 32 c - v .. of the padded row: T_i[v][32 c ..] = ref(i, 32 c - v ..);
+                        // chunks in batches of up to four, the batch's words loaded first
                         const int t0 = 128 + 32 * g.c0[vt] - (128 * vt + 32 * qd + lane);
                         const int sh = (t0 & 3) * 8;
                         const uint32_t *wp = row + (t0 >> 2);
-                        uint32_t p[9];
+                        for (int c = g.c0[vt]; c < g.c1[vt]; c += 4) {
+                            const int nb = min(4, g.c1[vt] - c);
+                            uint32_t p[33];
 #pragma unroll
-                        for (int j = 0; j < 9; ++j) p[j] = wp[j];
-                        for (int c = g.c0[vt]; c < g.c1[vt]; ++c, col += 8u) {
-                            uint32_t out[8];
+                            for (int j = 0; j < 33; ++j) p[j] = j <= 8 * nb ? wp[j] : 0u;
 #pragma unroll
-                            for (int j = 0; j < 8; ++j) out[j] = __funnelshift_r(p[j], p[j + 1], sh);
-                            i8::st8(col, out);
-                            if (c + 1 < g.c1[vt]) {
-                                wp += 8;
-                                p[0] = p[8];
+                            for (int q = 0; q < 4; ++q) {
+                                if (q < nb) {
+                                    uint32_t out[8];
 #pragma unroll
-                                for (int j = 1; j < 9; ++j) p[j] = wp[j];
+                                    for (int j = 0; j < 8; ++j) out[j] = __funnelshift_r(p[8 * q + j], p[8 * q + j + 1], sh);
+                                    i8::st8(col, out);
+                                    col += 8u;
+                                }
                             }
+                            wp += 8 * nb;
                         }
                     }
                     i8::st_wait();
@@ -572,65 +575,80 @@ __global__ void __launch_bounds__(kI8Threads, 1) corr_i8_kernel(I8Args args)
         }
     } else if (tid == kI8Mma) {
         // ---- the MMA issue: per group, per reference row, every K chunk of both lane tiles against
-        // every valid chip of the group, one ring stage (one wait, one commit)
-        const uint32_t idesc = i8_idesc(128, NU);
-        const uint32_t lbo16 = g.lbo >> 4;
-        int s = 0;
-        uint32_t round = 0;
+        // every valid chip of the group, one ring stage (one wait, one commit). Specialised on the
+        // frames per group so that between two MMAs there are only descriptor increments.
         bool ok = true;
-        auto valid_mask = [&](int gi) {
-            const int k = gi / gpw, f0 = (gi % gpw) * F, nfr = min(F, a.nf - f0);
-            unsigned m = 0;
-            for (int fi = 0; fi < nfr; ++fi)
-                if (i8::pair(a, k, f0 + fi).ok) m |= 1u << fi;
-            return m;
-        };
-        unsigned vm_next = int(blockIdx.x) < ngroups ? valid_mask(blockIdx.x) : 0u;
-        for (int gl = 0; ok; ++gl) {
-            const int gi = blockIdx.x + gl * gridDim.x;
-            if (gi >= ngroups) break;
-            const unsigned vm = vm_next;
-            const int cb = gl & 1, b = NB == 2 ? gl & 1 : 0;
-            if (!i8::wait(&bar_cfull[cb], uint32_t(gl >> 1) & 1u, abort) ||
-                (gl >= NB && !i8::wait(&bar_dempty[b], uint32_t((NB == 2 ? gl >> 1 : gl) - 1) & 1u, abort))) {
-                ok = false;
-                break;
-            }
-            tc::fence_after_sync();
-            if (vm) {
-                const uint32_t dbase = tmem + uint32_t(b * F * VT * NU);
-                uint64_t bdesc[4];
-#pragma unroll
-                for (int fi = 0; fi < 4; ++fi)
-                    bdesc[fi] = tc::smem_desc(tc::smem_u32(chips) + uint32_t(cb * F + (fi < F ? fi : 0)) * g.chip_bytes, g.lbo, 128);
-                for (int i = 0; i < W; ++i) {
-                    if (!i8::wait(&bar_full[s], round & 1u, abort)) {
-                        ok = false;
-                        break;
-                    }
-                    tc::fence_after_sync();
-                    uint32_t acol = tmem + g.ring_col + uint32_t(s) * g.stage_cols;
-                    for (int vt = 0; vt < VT; ++vt)
-                        for (int c = g.c0[vt]; c < g.c1[vt]; ++c, acol += 8u) {
-                            const uint32_t acc = (i | (c - g.c0[vt])) != 0 ? 1u : 0u;
-                            const uint64_t boff = uint64_t(uint32_t(2 * c) * lbo16 + uint32_t(i));
-#pragma unroll
-                            for (int fi = 0; fi < 4; ++fi)
-                                if (fi < F && (vm >> fi & 1u))
-                                    i8::mma(dbase + uint32_t((fi * VT + vt) * NU), acol, bdesc[fi] + boff, idesc, acc);
-                        }
-                    tc::mma_commit(&bar_empty[s]);
-                    if (++s == NS) {
-                        s = 0;
-                        ++round;
-                    }
+        auto issue = [&](auto FC) {
+            constexpr int FF = decltype(FC)::value;
+            const uint32_t idesc = i8_idesc(128, NU);
+            const uint32_t blk2 = 2u * (g.lbo >> 4);   // descriptor start units between two K chunks
+            int s = 0;
+            uint32_t round = 0;
+            auto valid_mask = [&](int gi) {
+                const int k = gi / gpw, f0 = (gi % gpw) * FF, nfr = min(FF, a.nf - f0);
+                unsigned m = 0;
+                for (int fi = 0; fi < nfr; ++fi)
+                    if (i8::pair(a, k, f0 + fi).ok) m |= 1u << fi;
+                return m;
+            };
+            unsigned vm_next = int(blockIdx.x) < ngroups ? valid_mask(blockIdx.x) : 0u;
+            for (int gl = 0; ok; ++gl) {
+                const int gi = blockIdx.x + gl * gridDim.x;
+                if (gi >= ngroups) break;
+                const unsigned vm = vm_next;
+                const int cb = gl & 1, b = NB == 2 ? gl & 1 : 0;
+                if (!i8::wait(&bar_cfull[cb], uint32_t(gl >> 1) & 1u, abort) ||
+                    (gl >= NB && !i8::wait(&bar_dempty[b], uint32_t((NB == 2 ? gl >> 1 : gl) - 1) & 1u, abort))) {
+                    ok = false;
+                    break;
                 }
-                if (!ok) break;
+                tc::fence_after_sync();
+                if (vm) {
+                    uint32_t dcol[FF];
+                    uint64_t bd[FF];
+#pragma unroll
+                    for (int fi = 0; fi < FF; ++fi) {
+                        dcol[fi] = tmem + uint32_t(((b * FF + fi) * VT) * NU);
+                        bd[fi] = tc::smem_desc(tc::smem_u32(chips) + uint32_t(cb * FF + fi) * g.chip_bytes, g.lbo, 128);
+                    }
+                    for (int i = 0; i < W; ++i) {
+                        if (!i8::wait(&bar_full[s], round & 1u, abort)) {
+                            ok = false;
+                            break;
+                        }
+                        tc::fence_after_sync();
+                        uint32_t acol = tmem + g.ring_col + uint32_t(s) * g.stage_cols;
+                        for (int vt = 0; vt < VT; ++vt) {
+                            const uint32_t dv = vt ? uint32_t(NU) : 0u;
+                            uint64_t bb[FF];
+#pragma unroll
+                            for (int fi = 0; fi < FF; ++fi) bb[fi] = bd[fi] + uint64_t(blk2 * uint32_t(g.c0[vt]) + uint32_t(i));
+                            for (int c = g.c0[vt]; c < g.c1[vt]; ++c) {
+                                const uint32_t acc = (i | (c - g.c0[vt])) != 0 ? 1u : 0u;
+#pragma unroll
+                                for (int fi = 0; fi < FF; ++fi) {
+                                    if (vm >> fi & 1u) i8::mma(dcol[fi] + dv, acol, bb[fi], idesc, acc);
+                                    bb[fi] += blk2;
+                                }
+                                acol += 8u;
+                            }
+                        }
+                        tc::mma_commit(&bar_empty[s]);
+                        if (++s == NS) {
+                            s = 0;
+                            ++round;
+                        }
+                    }
+                    if (!ok) break;
+                }
+                tc::mma_commit(&bar_dfull[b]);
+                tc::mma_commit(&bar_cempty[cb]);
+                if (gi + int(gridDim.x) < ngroups) vm_next = valid_mask(gi + gridDim.x);   // under this group's MMAs
             }
-            tc::mma_commit(&bar_dfull[b]);
-            tc::mma_commit(&bar_cempty[cb]);
-            if (gi + int(gridDim.x) < ngroups) vm_next = valid_mask(gi + gridDim.x);   // under this group's MMAs
-        }
+        };
+        if (F == 4) issue(std::integral_constant<int, 4>{});
+        else if (F == 2) issue(std::integral_constant<int, 2>{});
+        else issue(std::integral_constant<int, 1>{});
         if (!ok) *abort = 1;
         // nothing of this CTA's may still be running on the tensor core when TMEM is released
         tc::mma_commit(&bar_final);

@@ -136,7 +136,7 @@ def surfaces_vs_oracle(h, w, window, search, frames, gross=None, skip=24, limit=
 @pytest.mark.parametrize('window,search', [(3, 1), (11, 8), (32, 16), (64, 48), (45, 60), (64, 64), (128, 64),
                                            (100, 10)])
 def test_surfaces_geometries(window, search):
-    h, w = 300, 520
+    h, w = 420, 560
     frames = synth.video(h, w, 3, np.array([[0.0, 0.0], [1.3, -2.2], [-3.6, 2.9]]), np.zeros(3), sigma=2.0, noise=1.0,
                          seed=window * 7 + search)
     out, o = surfaces_vs_oracle(h, w, window, search, frames, skip=max(8, window // 2))
