@@ -99,17 +99,23 @@ class Clocks:
                 'samples': len(sm)}
 
 
-def profiled_traffic(form, fft_n):
-    """dram bytes per launch of the correlation kernel from the committed ncu summary of this
-    workload (profiles/corr_<form>_720p_w64_s48.md), or None"""
-    path = os.path.join(ROOT, 'profiles', f'corr_{form}_720p_w64_s48.md')
-    try:
-        for line in open(path):
-            if line.startswith('dram_bytes_per_launch:'):
-                return int(line.split(':')[1])
-    except OSError:
-        pass
-    return None
+# dram bytes per 16-frame launch of the correlation kernel (dram__bytes_read.sum + dram__bytes_write.sum
+# of one ncu capture of this workload; the captures and their commands are summarised in
+# profiles/corr_<form>_720p_w64_s48.md)
+TRAFFIC_PER_LAUNCH = {('fft32', 160): 328990464, ('tc', 160): 377420800}
+
+
+def dft_gemm_flops(n, m):
+    """useful DFT-GEMM work of one window (FFT size n, m shifts per axis), the scope table's formula:
+    forward row real DFT 4 n^2 (n/2+1) + column complex DFT 8 n^2 (n/2+1); inverse pruned to the m
+    output rows and columns, column 8 m n (n/2+1) + row 4 m^2 (n/2+1) (38.0 MFLOP at n = 160, m = 97)"""
+    nh = n // 2 + 1
+    return 4 * n * n * nh + 8 * n * n * nh + 8 * m * n * nh + 4 * m * m * nh
+
+
+def direct_ops(w, m):
+    """useful integer work of one window in the exact form: w^2 multiply-adds for each of m^2 shifts"""
+    return 2 * w * w * m * m
 
 
 def peaks():
@@ -214,6 +220,63 @@ def max_over_ranks(x, dist, device):
     return float(t.item())
 
 
+def accuracy(cor, frames, gross, gross_d, down, across, step_start, form, batch):
+    """The chosen form's offsets on the timed workload: every pair of one whole 16-frame step against
+    the FP32 form, and over 2,000 pairs against the FP64 direct-correlation oracle (frames 100, 110,
+    120 and 130, where the fault step ramps through 0 .. 40 px, and the step's first frame, on a
+    sub-grid of every second row and third column of windows), with the windows whose search region
+    straddles the fault line reported apart."""
+    import math
+
+    import torch
+
+    from oracle import oracle
+
+    def stats(d, snr_rel):
+        d = np.asarray(d, float)
+        return {'pairs': int(d.size), 'max_px': float(d.max()), 'p99_px': float(np.quantile(d, 0.99)),
+                'median_px': float(np.median(d)), 'frac_above_0.01px': float((d > 0.01).mean()),
+                'snr_rel_max': float(np.max(snr_rel)), 'snr_rel_p99': float(np.quantile(snr_rel, 0.99))}
+
+    out = {}
+    s = step_start
+    f, g = frames[s:s + batch], gross_d[s:s + batch]
+    a = cor.correlate(f, gross=g)
+    cor.set_form('fft32')
+    b = cor.correlate(f, gross=g)
+    cor.set_form(form)
+    ao, bo = a['offsets'].cpu().numpy(), b['offsets'].cpu().numpy()
+    valid = np.isfinite(bo[..., 0])
+    d = np.abs(ao - bo).max(-1)[valid]
+    mism = int((d > 0.5).sum())
+    snr = np.abs(a['snr'].cpu().numpy()[valid] / b['snr'].cpu().numpy()[valid] - 1)
+    ok = d <= 0.5
+    out['vs_fft32_whole_step'] = dict(stats(d[ok], snr[ok]), integer_peak_mismatches=mism,
+                                      frames=f"{s}..{s + batch - 1}")
+    pick = [100, 110, 120, 130, s]
+    fr = frames[pick].cpu().numpy()
+    gr = gross[pick]
+    ref0 = frames[0].cpu().numpy()
+    dsub, asub = down[::2], across[::3]
+    o = oracle.correlate(H, W_, dsub, asub, ref0, fr, gr, window=WIN, search=SEARCH, mode='f64')
+    r = cor.correlate(fr, gross=gr)
+    ro = r['offsets'][:, ::2, ::3]
+    valid = np.isfinite(o['offsets64'][..., 0])
+    d = np.abs(o['offsets64'] - ro).max(-1)
+    snr = np.abs(r['snr'][:, ::2, ::3] / np.where(valid, o['snr'], 1) - 1)
+    ok = valid & (d <= 0.5)
+    # the fault line of the synthetic video: 30 degrees through the frame centre
+    an = math.radians(30.0)
+    yc = np.asarray(dsub)[:, None] + WIN / 2.0 - H / 2.0
+    xc = np.asarray(asub)[None, :] + WIN / 2.0 - W_ / 2.0
+    straddle = np.abs(-xc * math.sin(an) + yc * math.cos(an)) <= (WIN + 2 * SEARCH) / 2.0
+    st = ok & straddle[None]
+    out['vs_fp64_oracle'] = dict(stats(d[ok], snr[ok]), integer_peak_mismatches=int((valid & (d > 0.5)).sum()),
+                                 frames=pick, windows='rows ::2, columns ::3 of the grid')
+    out['vs_fp64_oracle_fault_straddling'] = stats(d[st], snr[st]) if st.any() else None
+    return out
+
+
 def run_b200(args):
     import torch
     rank = int(os.environ.get('RANK', '0'))
@@ -243,6 +306,19 @@ def run_b200(args):
         s = starts[i]
         return cor.correlate(frames[s:s + BATCH], gross=gross_d[s:s + BATCH])
 
+    def device_rate(form):   # windows/s of a form on the timed steps (device time, this rank)
+        cor.set_form(form)
+        for i in range(2):
+            step_dev(i)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for i in range(args.steps):
+            step_dev(args.warmup + i)
+        e1.record()
+        torch.cuda.synchronize()
+        return world * args.steps * BATCH * nwin / (e0.elapsed_time(e1) / 1e3)
+
     for i in range(args.warmup):
         step_dev(i)
     torch.cuda.synchronize()
@@ -270,79 +346,86 @@ def run_b200(args):
     ms = max_over_ranks(ms, dist, 'cuda')
     value = world * args.steps * BATCH * nwin / (ms / 1e3)
 
-    # the other form on the same steps (device time), for comparison
-    other = 'fft32' if args.form in ('tc', 'int8') else 'tc'
-    cor.set_form(other)
-    for i in range(2):
-        step_dev(i)
-    torch.cuda.synchronize()
-    e0.record()
-    for i in range(args.steps):
-        step_dev(args.warmup + i)
-    e1.record()
-    torch.cuda.synchronize()
-    other_value = world * args.steps * BATCH * nwin / (e0.elapsed_time(e1) / 1e3)
+    # the other forms on the same steps (device time), for comparison
+    others = {}
+    for form in ('fft32', 'tc', 'int8'):
+        if form != args.form:
+            others[form] = device_rate(form)
     cor.set_form(args.form)
 
     if args.no_e2e:
-        print(json.dumps({'value': value, 'form': args.form, 'kernel_ms': kernel_ms, 'kernel_launches': kernel_launches,
-                          'other_form': other, 'other_value': other_value, 'clocks': clk}))
+        if rank == 0:
+            print(json.dumps({'value': value, 'form': args.form, 'kernel_ms': kernel_ms, 'kernel_launches': kernel_launches,
+                              'other_forms': others, 'clocks': clk}))
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
         return
-    # end to end through the host entry point: frames in page-locked memory, numpy outputs
+    # end to end through the host entry point, the way the reference's caller passes frames: a plain
+    # (pageable) numpy array; then the same from page-locked memory
     host = torch.empty(frames.shape, dtype=torch.uint8, pin_memory=True)
     host.copy_(frames)
-    host_np = host.numpy()
-    for i in range(2):
-        s = starts[i]
-        cor.correlate(host_np[s:s + BATCH], gross=gross[s:s + BATCH])
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t = time.perf_counter()
-    for i in range(args.steps):
-        s = starts[args.warmup + i]
-        r = cor.correlate(host_np[s:s + BATCH], gross=gross[s:s + BATCH])
-    e2e_s = time.perf_counter() - t
-    e2e_s = max_over_ranks(e2e_s, dist, 'cuda')
-    e2e = world * args.steps * BATCH * nwin / e2e_s
+    pinned_np = host.numpy()
+    pageable_np = np.array(pinned_np)   # an ordinary copy in pageable memory
 
-    # accuracy on one batch: offsets against the FP64 oracle on a sub-grid of windows
-    err = None
+    def e2e_rate(src):
+        for i in range(2):
+            s = starts[i]
+            cor.correlate(src[s:s + BATCH], gross=gross[s:s + BATCH])
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for i in range(args.steps):
+            s = starts[args.warmup + i]
+            cor.correlate(src[s:s + BATCH], gross=gross[s:s + BATCH])
+        dt = max_over_ranks(time.perf_counter() - t, dist, 'cuda')
+        return world * args.steps * BATCH * nwin / dt
+
+    e2e = e2e_rate(pageable_np)
+    e2e_pinned = e2e_rate(pinned_np)
+
+    acc = None
     cpu = None
     if rank == 0:
-        from oracle import oracle
-        s = starts[args.warmup]
-        fr = frames[s:s + 2].cpu().numpy()
-        ref0 = frames[0].cpu().numpy()
-        o = oracle.correlate(H, W_, down[::5], across[::7], ref0, fr, gross[s:s + 2], window=WIN, search=SEARCH,
-                             mode='f64')
-        b = cor.correlate(fr, gross=gross[s:s + 2])['offsets'][:, ::5, ::7]
-        ok = np.isfinite(o['offsets64'][..., 0])
-        d = np.abs(o['offsets64'] - b).max(-1)[ok]
-        err = float(np.median(d)), float(np.quantile(d, 0.99)), float((d > 0.01).mean())
+        acc = accuracy(cor, frames, gross, gross_d, down, across, starts[args.warmup], args.form, BATCH)
         if world == 1 and not args.no_cpu:
-            host_frames = host_np[:1 + args.cpu_frames]
-            cpu = reference_cpu(host_frames, gross, down, across, args.cpu_frames)
+            cpu = reference_cpu(pinned_np[:1 + args.cpu_frames], gross, down, across, args.cpu_frames)
 
     if rank == 0:
         pk = peaks()
-        sm_max = (clk or {}).get('sm_max_mhz') or pk.get('sm_max_mhz', 1965.0)
+        m = 2 * SEARCH + 1
         if args.form == 'tc':
-            bound, peak_v = 'tensor', pk.get('bf16_tflops', 1590.0)
+            bound, unit, peak_v = 'tensor', 'TFLOP/s', pk.get('bf16_tflops', 1590.0)
             peak_src = ('measured cuBLAS bf16 burst (MEASURED_PEAKS.json)' if 'bf16_tflops' in pk
                         else 'fallback 1.59 PFLOP/s')
-            work = tc_flops(fft_n, 2 * SEARCH + 1)
+            work = dft_gemm_flops(fft_n, m)
             kname = f'corr_tc_kernel<{fft_n}>'
+            executed = tc_flops(fft_n, m)
+        elif args.form == 'int8':
+            bound, unit = 'tensor', 'TOP/s'
+            peak_v = 2 * pk.get('bf16_tflops', 1590.0)
+            peak_src = ('twice the measured cuBLAS bf16 burst (MEASURED_PEAKS.json): the B200 int8 tensor rate is '
+                        'twice its bf16 rate')
+            work = direct_ops(WIN, m)
+            kname = 'corr_i8_kernel'
+            executed = 2 * 128 * ((m + 15) // 16 * 16) * ((WIN + 2 * SEARCH + 31) // 32 * 32) * WIN
         else:
-            bound, peak_v = 'fp32', 148 * 128 * 2 * sm_max * 1e6 / 1e12
+            sm_max = (clk or {}).get('sm_max_mhz') or pk.get('sm_max_mhz', 1965.0)
+            bound, unit, peak_v = 'fp32', 'TFLOP/s', 148 * 128 * 2 * sm_max * 1e6 / 1e12
             peak_src = 'nominal FP32 CUDA-core peak: 148 SMs x 128 lanes x 2 x max SM clock'
             work = fft_flops(fft_n)
             kname = f'corr_kernel<{fft_n}>'
+            executed = work
         achieved = work * pairs / (kernel_ms / 1e3) / 1e12 if kernel_ms > 0 else None
+        traffic = TRAFFIC_PER_LAUNCH.get((args.form, fft_n)) if BATCH == 16 else None
         out = {
             'metric': METRIC, 'value': value, 'unit': 'windows/s', 'n_gpus': world, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': ms / args.steps, 'higher_is_better': True, 'scaling': 'weak',
-            'vs_baseline': value / PUBLISHED_WPS, 'dtype': 'f16' if args.form == 'tc' else 'f32', 'data': 'synthetic',
+            'vs_baseline': value / PUBLISHED_WPS,
+            'dtype': {'tc': 'f16 operands, f32 accumulation', 'int8': 'u8 operands, s32 accumulation',
+                      'fft32': 'f32'}[args.form],
+            'data': 'synthetic',
             'config': {'workload': '720p video (300 frames), window 64, search 48, skip 16 (2450 windows/frame), '
                                    'per-frame gross = rounded camera motion',
                        'frames_per_step': BATCH, 'windows_per_step': BATCH * nwin, 'fft_size': fft_n,
@@ -350,19 +433,24 @@ def run_b200(args):
                        'l2': 'per step: 254 MB of resident reference spectra + 14.7 MB of frames read '
                              '(> 126 MB L2); the batches walk through a 276 MB video'},
             'e2e': {'value': e2e, 'unit': 'windows/s', 'h2d_bytes_per_step': BATCH * H * W_ + BATCH * 2 * 4,
-                    'd2h_bytes_per_step': BATCH * nwin * 7 * 4},
+                    'd2h_bytes_per_step': BATCH * nwin * 7 * 4,
+                    'input': 'pageable numpy frames (as track_offsets passes them), outputs in numpy arrays'},
+            'e2e_pinned': {'value': e2e_pinned, 'unit': 'windows/s', 'input': 'frames in page-locked host memory'},
             'gpu_launches': launches,
-            'roofline': {'bound': bound, 'achieved': achieved, 'peak': peak_v, 'unit': 'TFLOP/s',
+            'roofline': {'bound': bound, 'achieved': achieved, 'peak': peak_v, 'unit': unit,
                          'frac': (achieved / peak_v) if achieved else None,
-                         'traffic': profiled_traffic(args.form, fft_n) if BATCH == 16 else None,
-                         'traffic_source': 'ncu dram__bytes_read.sum + dram__bytes_write.sum of one 16-frame launch '
-                                           f'(profiles/corr_{args.form}_720p_w64_s48.md)',
+                         'traffic': traffic,
+                         'traffic_source': f'ncu dram bytes of one 16-frame launch of {kname}'
+                                           f' (profiles/corr_{args.form}_720p_w64_s48.md)' if traffic else None,
                          'kernel': kname, 'kernel_ms_per_launch': kernel_ms / max(kernel_launches, 1),
-                         'peak_source': peak_src, 'flop_per_window': work,
+                         'peak_source': peak_src, 'work_per_window': work, 'executed_per_window': executed,
+                         'work_source': {'tc': 'useful DFT-GEMM FLOPs, one pass (forward 4n^2 nh + 8n^2 nh, '
+                                                'inverse 8 m n nh + 4 m^2 nh)',
+                                         'int8': 'useful integer ops of the direct correlation, 2 W^2 M^2',
+                                         'fft32': 'useful FFT FLOPs 2 x 2.5 n^2 log2 n^2 + 6 n nh'}[args.form],
                          'useful_fft_flop_per_window': fft_flops(fft_n)},
-            'other_form': {'form': other, 'value': other_value, 'unit': 'windows/s'},
-            'accuracy': None if err is None else {'vs': 'FP64 direct-correlation oracle, 2 frames, 7 x 10 windows',
-                                                  'median_px': err[0], 'p99_px': err[1], 'frac_above_0.01px': err[2]},
+            'other_forms': {k: {'value': v, 'unit': 'windows/s'} for k, v in others.items()},
+            'accuracy': acc,
             'clocks': clk,
         }
         if cpu is not None:
@@ -742,6 +830,60 @@ def run_scans(args):
     }))
 
 
+def launch_ranks(n):
+    """--gpus N without a launcher: start N ranks of this same command through torch.distributed.run
+    (one process per GPU, rendezvous on 127.0.0.1) and return its exit code. N above the visible
+    device count is refused with a message."""
+    import socket
+
+    try:
+        import torch
+        if torch.cuda.is_available() and n > torch.cuda.device_count():
+            print(f'bench.py: --gpus {n} but {torch.cuda.device_count()} CUDA device(s) are visible', file=sys.stderr)
+            return 2
+    except ImportError:
+        pass
+    with socket.socket() as sk:   # a free port for the rendezvous
+        sk.bind(('127.0.0.1', 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, '-m', 'torch.distributed.run', '--nnodes=1', f'--nproc-per-node={n}', '--master-addr',
+           '127.0.0.1', '--master-port', str(port), os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.run(cmd).returncode
+
+
+def run_launch_check(args):
+    """The multi-rank plumbing alone (no GPU needed): every rank joins the process group (gloo without
+    CUDA), takes its batches with shard_starts, times a small host computation, and rank 0 prints the
+    line with the max over ranks, as the correlation workload does."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    if world > 1:
+        dist.init_process_group('nccl' if torch.cuda.is_available() else 'gloo', timeout=datetime.timedelta(seconds=60))
+    starts = shard_starts(rank, world, NFRAMES, BATCH, args.steps)
+    t = time.perf_counter()
+    a = np.random.default_rng(rank).random((256, 256))
+    for _ in range(args.steps):
+        a = a @ a.T / 256.0
+    dt = time.perf_counter() - t
+    dev = 'cuda' if torch.cuda.is_available() else 'cpu'
+    slowest = max_over_ranks(dt, dist if world > 1 else None, dev)
+    seen = [None] * world
+    if world > 1:
+        dist.all_gather_object(seen, {'rank': rank, 'first_batch': starts[0]})
+    else:
+        seen = [{'rank': 0, 'first_batch': starts[0]}]
+    if rank == 0:
+        print(json.dumps({'metric': 'launch check', 'n_gpus': world, 'ranks': seen, 'value': world * args.steps / slowest,
+                          'unit': 'steps/s', 'steps': args.steps}))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     p.add_argument('--gpus', type=int, default=1)
@@ -754,12 +896,17 @@ def main():
     p.add_argument('--video', type=int, default=NFRAMES, help='frames of the synthetic video to render')
     p.add_argument('--batch', type=int, default=BATCH, help='frames per step')
     p.add_argument('--form', default='tc', choices=['fft32', 'tc', 'int8'], help='the arithmetic of the transforms')
-    p.add_argument('--workload', default='hd', choices=['hd', 'mixed', 'stream', 'diff', 'stabilize', 'scans'],
+    p.add_argument('--workload', default='hd', choices=['hd', 'mixed', 'stream', 'diff', 'stabilize', 'scans',
+                                                       'launch-check'],
                    help='hd: the 720p headline; mixed: three grids in one group step; stream: 1080p streaming; '
                         'diff: the differentiable path; stabilize: coarse similarity tracking; '
                         'scans: frame differences, text mask, periodicity')
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.gpus > 1 and 'WORLD_SIZE' not in os.environ:
+        sys.exit(launch_ranks(args.gpus))
+    if args.workload == 'launch-check':
+        return run_launch_check(args)
     if args.workload == 'mixed' and args.impl != 'reference':
         run_mixed(args)
     elif args.workload == 'stream' and args.impl != 'reference':

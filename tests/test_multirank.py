@@ -74,3 +74,21 @@ def test_shard_starts_one_rank_and_errors():
     assert bench.max_over_ranks(3.5, None, 'cpu') == 3.5
     with pytest.raises(ValueError):
         bench.shard_starts(0, 1, 10, 16, 1)
+
+
+def test_bench_launches_its_own_ranks():
+    """bench.py --gpus 2 without a launcher starts two ranks itself (torch.distributed.run, gloo here
+    without a GPU); both ran, took disjoint batches, and the line reports n_gpus 2."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ('RANK', 'WORLD_SIZE', 'LOCAL_RANK', 'MASTER_ADDR', 'MASTER_PORT')}
+    env['CUDA_VISIBLE_DEVICES'] = ''
+    r = subprocess.run([sys.executable, os.path.join(root, 'bench.py'), '--gpus', '2', '--workload', 'launch-check',
+                        '--steps', '3'], capture_output=True, text=True, timeout=240, env=env, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith('{')][-1])
+    assert line['n_gpus'] == 2
+    assert sorted(x['rank'] for x in line['ranks']) == [0, 1]
+    assert len({x['first_batch'] for x in line['ranks']}) == 2
