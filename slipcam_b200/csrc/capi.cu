@@ -27,6 +27,7 @@
 #include "corr_big.cuh"
 #include "corr_tc.cuh"
 #include "corr_i8.cuh"
+#include "refine.cuh"
 #include "diff.h"
 #include "multi.h"
 #include "periodicity.cuh"
@@ -104,7 +105,8 @@ struct Slot {
     DevBuf<uint32_t> sat;
     DevBuf<int64_t> sat2;
     DevBuf<float> dinv;
-    DevBuf<int2> bstat;         // {box sum, dinv} beside dinv (the exact tensor-core form)
+    DevBuf<int2> bstat;         // {box sum, dinv} beside dinv (the exact tensor-core form, the refinement)
+    DevBuf<PeakInfo> peaks;     // the tensor-core kernel's peaks, for their exact refinement
     DevBuf<int32_t> gross;
     DevBuf<float> out;          // offset 2P | peak P | snr P | cov 3P, P = group * nwin
     HostBuf<uint8_t> hframes;
@@ -446,6 +448,7 @@ struct b200_handle {
     DevBuf<uint8_t> d_refwin;    // the exact tensor-core form: the reference windows' pixels, nwin x W x W
     DevBuf<int> d_sref;          // and their sums
     DevBuf<int2> d_bstat;        // device-path box table (beside d_dinv)
+    DevBuf<PeakInfo> d_peaks;    // device-path peaks of the tensor-core form
     DevBuf<uint32_t> d_sat;      // device-path scratch
     DevBuf<int64_t> d_sat2;
     DevBuf<float> d_dinv;
@@ -502,6 +505,10 @@ struct b200_handle {
             s.sat2.alloc(G * sat_size());
             s.dinv.alloc(G * dinv_size());
             if (i8_ok) s.bstat.alloc(G * dinv_size());
+            if (i8_ok && tc_ok) {
+                s.peaks.alloc(P);
+                CK(cudaMemset(s.peaks.p, 0, P * sizeof(PeakInfo)));
+            }
             s.gross.alloc(2 * P);
             s.out.alloc(7 * P);
             s.hframes.alloc(G * height * fpitch);
@@ -528,6 +535,10 @@ struct b200_handle {
         d_sat2.alloc(G * sat_size());
         d_dinv.alloc(G * dinv_size());
         if (i8_ok) d_bstat.alloc(G * dinv_size());
+        if (i8_ok && tc_ok) {
+            d_peaks.alloc(G * nwin);
+            CK(cudaMemset(d_peaks.p, 0, G * nwin * sizeof(PeakInfo)));
+        }
         if (tc_ok) {
             const CUtensorMap m = dinv_map(d_dinv.p, height, width, dpitch(), int(G), M);
             CK(cudaMemcpy(d_tmaps.p + 2, &m, sizeof(m), cudaMemcpyHostToDevice));
@@ -537,14 +548,23 @@ struct b200_handle {
     // the tables and the correlation of nf frames (device memory) on stream s; bstat (the box table
     // beside dinv) serves the exact tensor-core form
     void run_group(const uint8_t *frames, int pitch, int nf, const int32_t *gross, int gross_mode,
-                   uint32_t *sat, int64_t *sat2, float *dinv, int2 *bstat, float *offset, float *peak, float *snr,
-                   float *cov, float *surface, cudaStream_t s)
+                   uint32_t *sat, int64_t *sat2, float *dinv, int2 *bstat, PeakInfo *peaks, float *offset, float *peak,
+                   float *snr, float *cov, float *surface, cudaStream_t s)
     {
         const int arith = form != B200_FORM_I8 ? form : (bstat && ref_u8) ? B200_FORM_I8 : B200_FORM_FFT32;
-        run_tables(frames, pitch, nf, sat, sat2, dinv, s, arith == B200_FORM_I8 ? bstat : nullptr);
+        // the tensor-core form's peaks are refined exactly where the reference windows are at hand
+        const bool refine = arith == B200_FORM_TC && peaks && bstat && ref_u8;
+        run_tables(frames, pitch, nf, sat, sat2, dinv, s, arith == B200_FORM_I8 || refine ? bstat : nullptr);
         CorrArgs a = corr_args(frames, pitch, nf, gross, gross_mode, sat, dinv, offset, peak, snr, cov, surface);
         a.bstat = bstat;
+        a.peaks = refine ? peaks : nullptr;
         run_corr_tail(a, nf, dinv, arith, s);
+        if (refine) {
+            const int64_t threads = int64_t(nf) * nwin * 32;
+            tc_refine_kernel<<<unsigned((threads + 255) / 256), 256, 0, s>>>(a, d_refwin.p, d_sref.p);
+            CK(cudaGetLastError());
+            launches += 1;
+        }
         launches += 3;
     }
 
@@ -988,7 +1008,7 @@ int b200_correlate(b200_handle *h, const uint8_t *frames, int n, const int32_t *
             CK(cudaEventRecord(s.in, h->copy));
             CK(cudaStreamWaitEvent(h->comp, s.in, 0));
             float *o = s.out.p;
-            h->run_group(s.frames.p, h->fpitch, nf, dg, gross_mode, s.sat.p, s.sat2.p, s.dinv.p, s.bstat.p, o, o + 2 * PG,
+            h->run_group(s.frames.p, h->fpitch, nf, dg, gross_mode, s.sat.p, s.sat2.p, s.dinv.p, s.bstat.p, s.peaks.p, o, o + 2 * PG,
                          o + 3 * PG, o + 4 * PG, nullptr, h->comp);
             CK(cudaMemcpyAsync(s.hout.p, s.out.p, 7 * PG * sizeof(float), cudaMemcpyDeviceToHost, h->comp));
             CK(cudaEventRecord(s.done, h->comp));
@@ -1025,7 +1045,7 @@ static int correlate_device(b200_handle *h, const uint8_t *frames, int n, int pi
             const size_t q0 = size_t(f0) * nwin;
             const int32_t *g = gross_mode == B200_GROSS_FRAME ? gross + 2 * size_t(f0)
                              : gross_mode == B200_GROSS_WINDOW ? gross + 2 * q0 : nullptr;
-            h->run_group(frames + f0 * fstride, pitch, nf, g, gross_mode, h->d_sat.p, h->d_sat2.p, h->d_dinv.p, h->d_bstat.p,
+            h->run_group(frames + f0 * fstride, pitch, nf, g, gross_mode, h->d_sat.p, h->d_sat2.p, h->d_dinv.p, h->d_bstat.p, h->d_peaks.p,
                          offset + 2 * q0, peak + q0, snr + q0, cov + 3 * q0,
                          surface ? surface + q0 * size_t(h->M) * h->M : nullptr, s);
         }

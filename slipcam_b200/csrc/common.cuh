@@ -43,6 +43,15 @@ struct SpectraArgs {
     const float2 *twiddles;    // 2N: the twiddle tables of the N-point transform
 };
 
+// what the tensor-core kernel leaves for the exact refinement of a pair's peak: the integer peak,
+// the SNR patch's count and sum of squares, and the 3 x 3 values around the peak it used
+struct PeakInfo {
+    int valid, u, v, count;
+    double sum;
+    float fit[9];
+    int pad;
+};
+
 // the arguments of the correlation kernels: one group of nf frames
 struct CorrArgs {
     const uint8_t *frames;     // nf frames, `pitch` bytes per row, `fstride` bytes per frame
@@ -67,6 +76,7 @@ struct CorrArgs {
                                // surface ((NaN, NaN, -inf) for an invalid pair)
     const int2 *bstat;         // nullptr, or nf x h x dpitch: {pixel sum, dinv bits} of each W x W box
                                // (the exact tensor-core form's table, beside dinv)
+    PeakInfo *peaks;           // nullptr, or nf x nwin: the tensor-core kernel's peaks for refinement
 };
 
 }   // namespace b200

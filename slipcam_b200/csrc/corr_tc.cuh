@@ -420,12 +420,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
         e_pv = s_peak[2];
         if (!e_valid) {
             invalid_outputs(prev.q, a.offset, a.peak, a.snr, a.cov);
+            if (a.peaks) a.peaks[prev.q].valid = 0;
             return;
         }
         int i0, i1, j0, j1;
         snr_patch(M, a.stat, e_pu, e_pv, i0, i1, j0, j1);
         double sum = 0.0;
         for (int w = 0; w < kTcCompute; ++w) sum += s_sq[w];
+        if (a.peaks) {   // for the exact refinement of the peak (tc_refine_kernel)
+            PeakInfo &pi = a.peaks[prev.q];
+            pi.valid = 1;
+            pi.u = e_pu;
+            pi.v = e_pv;
+            pi.count = (i1 - i0) * (j1 - j0);
+            pi.sum = sum;
+            for (int t = 0; t < 9; ++t) pi.fit[t] = s_fit[t];
+        }
         peak_outputs(s_fit + 4, 3, M, e_pu, e_pv, R, prev.gy, prev.gx, W * W, sum, (i1 - i0) * (j1 - j0), prev.q,
                      a.offset, a.peak, a.snr, a.cov);
     };
@@ -450,7 +460,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
     bool failed = false;
     while (cur.p < npairs) {
         if (!cur.ok) {   // an invalid pair: its outputs now (the pending epilogue waits)
-            if (ctrl) invalid_outputs(cur.q, a.offset, a.peak, a.snr, a.cov);
+            if (ctrl) {
+                invalid_outputs(cur.q, a.offset, a.peak, a.snr, a.cov);
+                if (a.peaks) a.peaks[cur.q].valid = 0;
+            }
             if (a.surface)
                 for (int i = tid; i < M * M; i += NT) a.surface[cur.q * M * M + i] = 0.0f;
             if (ctrl) s_next = pair_setup(cur.p + gridDim.x);

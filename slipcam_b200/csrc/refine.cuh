@@ -1,0 +1,128 @@
+// refine.cuh -- the exact refinement of the tensor-core form's peaks. The FP16 DFT-GEMMs leave an
+// error of about 3e-4 in each surface value; the sub-pixel offset, the peak value and the
+// covariance are read from the 3 x 3 values around the peak alone (cxx/surface.h:71-146), so this
+// kernel recomputes those nine values exactly -- the integer correlation sum_ij ref(i, j) x(i + u,
+// j + v) of the reference window and the frame in 32-bit integers, normalized as the exact form does
+// (i8::rho) -- replaces them in the SNR patch's sum of squares, and writes the pair's outputs again.
+// When an exact neighbour is larger than the peak (the FP16 argmax fell on the wrong side of a tie
+// between adjacent shifts), the peak climbs to it and the SNR patch around the new peak is summed
+// exactly; so is the patch of windows up to 32 px, whose small surfaces weigh the FP16 errors more
+// in the SNR. One warp per pair, the reference rows shared between the lanes.
+#pragma once
+
+#include "corr_i8.cuh"
+
+namespace b200 {
+
+#ifdef __CUDACC__
+
+// the exact integer correlation at shift (u, v) of the chip, summed over the warp (every lane gets it)
+__device__ __forceinline__ int exact_srx(const uint8_t *chip, int64_t pitch, const uint8_t *ref, int W, int u, int v, int lane)
+{
+    int acc = 0;
+    for (int i = lane; i < W; i += 32) {
+        const uint8_t *rr = ref + size_t(i) * W, *cr = chip + int64_t(u + i) * pitch + v;
+        for (int j = 0; j < W; ++j) acc += int(uint32_t(__ldg(rr + j)) * uint32_t(__ldg(cr + j)));
+    }
+    for (int d = 16; d > 0; d >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, d);
+    return acc;
+}
+
+__global__ void __launch_bounds__(256) tc_refine_kernel(CorrArgs a, const uint8_t *refwin, const int *sref)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t p = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;   // the pair (its output index)
+    if (p >= int64_t(a.nwin) * a.nf) return;
+    const PeakInfo &pi = a.peaks[p];
+    const int k = int(p % a.nwin), f = int(p / a.nwin);
+    const i8::Pair o = i8::pair(a, k, f);
+    const int W = a.W, M = a.M, L = a.L, n = W * W;
+    // only pairs the tensor-core kernel found a peak for (the search window inside the frame)
+    if (!o.ok || !pi.valid || pi.u < 0 || pi.u >= M || pi.v < 0 || pi.v >= M) return;
+    const uint8_t *chip = a.frames + o.f * a.fstride + int64_t(o.sy) * a.pitch + o.sx;
+    const uint8_t *ref = refwin + size_t(k) * W * W;
+    const float scale = float(1.0 / (double(n) * double(a.norm[k])));
+    const int2 *bt0 = a.bstat + size_t(o.f) * a.dinv_fstride + size_t(o.sy) * a.dpitch + o.sx;
+    const int sr = sref[k];
+    int pu = pi.u, pv = pi.v;
+    float fit[9];
+    int u0 = 0, u1 = 0, v0 = 0, v1 = 0;
+    bool moved = false;
+    for (int step = 0; step < 8; ++step) {
+        u0 = pu > 0 ? -1 : 0;   // the neighbours inside the surface
+        u1 = pu < M - 1 ? 1 : 0;
+        v0 = pv > 0 ? -1 : 0;
+        v1 = pv < M - 1 ? 1 : 0;
+        int s[3][3] = {};
+        for (int i = lane; i < W; i += 32) {
+            const uint8_t *rr = ref + size_t(i) * W;
+            for (int du = u0; du <= u1; ++du) {
+                // chip row pu + du + i, columns pv + v0 .. pv + v1 + W - 1 (all inside [0, L))
+                const uint8_t *cr = chip + int64_t(pu + du + i) * a.pitch + pv;
+                int sm = 0, s0 = 0, sp = 0;
+                uint32_t bm = v0 < 0 ? __ldg(cr - 1) : 0u, b0 = __ldg(cr);
+                for (int j = 0; j < W; ++j) {
+                    const uint32_t x = __ldg(rr + j);
+                    const uint32_t bp = (v1 > 0 || j + 1 < W) && pv + j + 1 < L ? __ldg(cr + j + 1) : 0u;
+                    sm += int(x * bm);
+                    s0 += int(x * b0);
+                    sp += int(x * bp);
+                    bm = b0;
+                    b0 = bp;
+                }
+                s[du + 1][0] += sm;
+                s[du + 1][1] += s0;
+                s[du + 1][2] += sp;
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < 9; ++t)
+            for (int d = 16; d > 0; d >>= 1) s[t / 3][t % 3] += __shfl_xor_sync(0xffffffffu, s[t / 3][t % 3], d);
+        // the exact values, and the best of the 3 x 3 (the reference's rule: the larger, the first in
+        // raster order if equal); every lane computes the same
+        float best = -2.0f;
+        int bu = pu, bv = pv, bat = INT_MAX;
+        for (int du = u0; du <= u1; ++du)
+            for (int dv = v0; dv <= v1; ++dv) {
+                const int t = (du + 1) * 3 + dv + 1;
+                const int2 st = __ldg(bt0 + int64_t(pu + du) * a.dpitch + pv + dv);
+                fit[t] = i8::rho(uint32_t(s[du + 1][dv + 1]), st, n, sr, scale);
+                const int at = (pu + du) * M + pv + dv;
+                if (fit[t] > best || (fit[t] == best && at < bat)) {
+                    best = fit[t];
+                    bat = at;
+                    bu = pu + du;
+                    bv = pv + dv;
+                }
+            }
+        if ((bu == pu && bv == pv) || step == 7) break;   // fit[] holds the values around (pu, pv)
+        pu = bu;   // a neighbour is the larger: the FP16 argmax was an adjacent near-tie
+        pv = bv;
+        moved = true;
+    }
+    int i0, i1, j0, j1;
+    snr_patch(M, a.stat, pu, pv, i0, i1, j0, j1);
+    double sum = 0.0;
+    if (!moved && W > 32) {   // the tensor-core patch with its 3 x 3 replaced
+        sum = pi.sum;
+        for (int du = u0; du <= u1; ++du)
+            for (int dv = v0; dv <= v1; ++dv) {
+                const int t = (du + 1) * 3 + dv + 1;
+                sum += double(fit[t]) * double(fit[t]) - double(pi.fit[t]) * double(pi.fit[t]);
+            }
+    } else {        // a new patch, or a small window's (cheap, and its FP16 errors weigh more): all exact
+        for (int u = i0; u < i1; ++u)
+            for (int v = j0; v < j1; ++v) {
+                const int srx = exact_srx(chip, a.pitch, ref, W, u, v, lane);
+                const float x = i8::rho(uint32_t(srx), __ldg(bt0 + int64_t(u) * a.dpitch + v), n, sr, scale);
+                sum += double(x) * double(x);
+            }
+    }
+    if (lane != 0) return;
+    peak_outputs(fit + 4, 3, M, pu, pv, a.R, o.gy, o.gx, n, sum, (i1 - i0) * (j1 - j0), p, a.offset, a.peak, a.snr,
+                 a.cov);
+}
+
+#endif   // __CUDACC__
+
+}   // namespace b200
