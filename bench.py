@@ -222,7 +222,8 @@ def max_over_ranks(x, dist, device):
 
 def accuracy(cor, frames, gross, gross_d, down, across, step_start, form, batch):
     """The chosen form's offsets on the timed workload: every pair of one whole 16-frame step against
-    the FP32 form, and over 2,000 pairs against the FP64 direct-correlation oracle (frames 100, 110,
+    the exact integer form (whose offsets are the FP64 oracle's within 1e-4 px on every golden case)
+    and the FP32 form, and over 2,000 pairs against the FP64 direct-correlation oracle (frames 100, 110,
     120 and 130, where the fault step ramps through 0 .. 40 px, and the step's first frame, on a
     sub-grid of every second row and third column of windows), with the windows whose search region
     straddles the fault line reported apart."""
@@ -241,18 +242,21 @@ def accuracy(cor, frames, gross, gross_d, down, across, step_start, form, batch)
     out = {}
     s = step_start
     f, g = frames[s:s + batch], gross_d[s:s + batch]
+
+    def versus(a, b):   # a against b on every pair of the step that b finds valid
+        ao, bo = a['offsets'].cpu().numpy(), b['offsets'].cpu().numpy()
+        valid = np.isfinite(bo[..., 0])
+        d = np.abs(ao - bo).max(-1)[valid]
+        snr = np.abs(a['snr'].cpu().numpy()[valid] / b['snr'].cpu().numpy()[valid] - 1)
+        ok = d <= 0.5
+        return dict(stats(d[ok], snr[ok]), integer_peak_mismatches=int((d > 0.5).sum()), frames=f'{s}..{s + batch - 1}')
+
     a = cor.correlate(f, gross=g)
-    cor.set_form('fft32')
-    b = cor.correlate(f, gross=g)
+    for ref_form in ('int8', 'fft32'):   # the exact integer form (the FP64 oracle's results to 1e-4 px), FP32
+        if ref_form != form:
+            cor.set_form(ref_form)
+            out[f'vs_{ref_form}_whole_step'] = versus(a, cor.correlate(f, gross=g))
     cor.set_form(form)
-    ao, bo = a['offsets'].cpu().numpy(), b['offsets'].cpu().numpy()
-    valid = np.isfinite(bo[..., 0])
-    d = np.abs(ao - bo).max(-1)[valid]
-    mism = int((d > 0.5).sum())
-    snr = np.abs(a['snr'].cpu().numpy()[valid] / b['snr'].cpu().numpy()[valid] - 1)
-    ok = d <= 0.5
-    out['vs_fft32_whole_step'] = dict(stats(d[ok], snr[ok]), integer_peak_mismatches=mism,
-                                      frames=f"{s}..{s + batch - 1}")
     pick = [100, 110, 120, 130, s]
     fr = frames[pick].cpu().numpy()
     gr = gross[pick]

@@ -50,7 +50,9 @@ extern "C" {
 #define B200_GROSS_WINDOW 2
 
 /* the arithmetic of the transforms */
-#define B200_FORM_AUTO 0   /* the library's choice */
+#define B200_FORM_AUTO 0   /* the library's choice, and the default: B200_FORM_TC for windows above 32 px
+                              where it holds the geometry (FFT size up to 160, search up to 63 px),
+                              else B200_FORM_FFT32 */
 #define B200_FORM_FFT32 1  /* FP32 FFTs on the CUDA cores */
 #define B200_FORM_TC 2     /* DFT-matrix GEMMs on the tensor cores, FP16 operands, FP32 accumulation */
 #define B200_FORM_I8 3     /* direct correlation on the tensor cores in exact integers (uint8 x uint8,

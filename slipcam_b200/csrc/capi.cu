@@ -810,6 +810,13 @@ void b200::tc_dft_table(int N, uint16_t *out)
 
 extern "C" {
 
+// the library's choice: the tensor-core form (its peaks refined exactly) where it holds the geometry
+// and is the faster -- windows above 32 px -- else the FP32 form
+static int auto_form(const b200_handle *h)
+{
+    return h->tc_ok && h->i8_ok && h->W > 32 ? B200_FORM_TC : B200_FORM_FFT32;
+}
+
 int b200_create(const b200_params *p, int device, b200_handle **out)
 {
     if (out) *out = nullptr;
@@ -878,6 +885,7 @@ int b200_create(const b200_params *p, int device, b200_handle **out)
         }
         // the maps of the two slots and of the device path's table are written when those are allocated
         if (h->tc_ok) h->d_tmaps.alloc(3);
+        h->form = auto_form(h);
         *out = h;
         g_create_error.clear();
         return B200_OK;
@@ -916,7 +924,7 @@ int b200_set_form(b200_handle *h, int form)
             fail(B200_EINVAL, "the exact tensor-core form holds windows up to " + std::to_string(kI8MaxWindow)
                                   + " px and search windows up to 256 px, not " + std::to_string(h->W) + " and "
                                   + std::to_string(h->L));
-        h->form = form == B200_FORM_AUTO ? B200_FORM_FFT32 : form;
+        h->form = form == B200_FORM_AUTO ? auto_form(h) : form;
     });
 }
 

@@ -31,6 +31,7 @@ class DiffCorrelator:
     def __init__(self, height, width, down, across, *, window=64, search=48, stat_size=21, device=0):
         self.cor = framecor.Correlator(height, width, down, across, window=window, search=search,
                                        backend='b200', stat_size=stat_size, device=device)
+        self.cor.set_form('fft32')   # the float frames' passes are the FP32 form's
         self.height, self.width = height, width
         self.ny, self.nx = self.cor.shape
         self.window, self.search = window, search

@@ -274,6 +274,7 @@ def periodicity(ref, y0, x0, window, search, exclude=5):
     f = f.to(torch.uint8).cuda().contiguous()
     h, w = f.shape
     cor = Correlator(h, w, y0, x0, window=window, search=search, backend='b200')
+    cor.set_form('fft32')   # surfaces to the FP32 form's accuracy
     cor.set_reference(f)
     surf = cor.correlate(f[None], surfaces=True)['surface']
     ny, nx = cor.shape

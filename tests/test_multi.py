@@ -38,6 +38,7 @@ def singles(ref, frames, gross):
     out = []
     for g, gg in zip(grids(), gross):
         c = framecor.Correlator(H, W, g['down'], g['across'], window=g['window'], search=g['search'], backend='b200')
+        c.set_form('fft32')   # the group's arithmetic
         c.set_reference(ref)
         out.append(c.correlate(torch.as_tensor(frames).cuda(), gross=None if gg is None else torch.as_tensor(gg).cuda()))
     return out

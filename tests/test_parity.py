@@ -261,6 +261,7 @@ def test_tc_fp64_oracle(name):
 def test_tc_surfaces_close_to_fft32():
     c = cases.case('hd')
     cor = framecor.Correlator(c['height'], c['width'], c['down'], c['across'], window=64, search=48, backend='b200')
+    cor.set_form('fft32')
     cor.set_reference(c['reference'])
     f = torch.as_tensor(c['frames']).cuda()
     g = torch.as_tensor(c['gross']).cuda()

@@ -2,7 +2,8 @@
 The no-allocation entry point, b200_correlate_device_noalloc, for callers that cannot allocate
 device memory while they correlate (a capture loop that must not stall on cudaMalloc, a host that
 owns all device memory). It keeps its per-frame tables in a static device array instead of the
-handle's buffers; its outputs must match b200_correlate_device's, call after call.
+handle's buffers; it always runs the FP32 form, and its outputs must match b200_correlate_device's
+with that form, call after call, at the FFT sizes 160, 192 and 256 (the big transform's clusters).
 
 This file is collected last on purpose (pytest -x stops at it only after every other test ran).
 """
@@ -41,12 +42,14 @@ def same(a, b):
         assert np.abs(x[ok] - y[ok]).max(initial=0.0) <= TOL
 
 
-def test_noalloc_matches_device_entry_point():
+@pytest.mark.parametrize('window, search, skip', [(64, 48, 16), (64, 64, 48), (128, 64, 64)])
+def test_noalloc_matches_device_entry_point(window, search, skip):
     """Two calls in a row on different frames: each matches the allocating entry point."""
     frames, motion, step, gross = synth.hd(n=12, count=12, device='cuda')
     g = torch.as_tensor(gross).cuda()
-    down, across = framecor.window_grid(720, 1280, 64, 48, 16)
-    cor = framecor.Correlator(720, 1280, down, across, window=64, search=48, backend='b200')
+    down, across = framecor.window_grid(720, 1280, window, search, skip)
+    cor = framecor.Correlator(720, 1280, down, across, window=window, search=search, backend='b200')
+    cor.set_form('fft32')   # the form the no-allocation entry point runs
     cor.set_reference(frames[0])
     for first, last in ((1, 6), (6, 12)):
         f, gg = frames[first:last].contiguous(), g[first:last].contiguous()
