@@ -107,6 +107,7 @@ struct Slot {
     DevBuf<float> dinv;
     DevBuf<int2> bstat;         // {box sum, dinv} beside dinv (the exact tensor-core form, the refinement)
     DevBuf<PeakInfo> peaks;     // the tensor-core kernel's peaks, for their exact refinement
+    DevBuf<int> queue;          // the refinement's pairs whose SNR patch is summed exactly (count first)
     DevBuf<int32_t> gross;
     DevBuf<float> out;          // offset 2P | peak P | snr P | cov 3P, P = group * nwin
     HostBuf<uint8_t> hframes;
@@ -449,6 +450,7 @@ struct b200_handle {
     DevBuf<int> d_sref;          // and their sums
     DevBuf<int2> d_bstat;        // device-path box table (beside d_dinv)
     DevBuf<PeakInfo> d_peaks;    // device-path peaks of the tensor-core form
+    DevBuf<int> d_queue;         // and the refinement's queue
     DevBuf<uint32_t> d_sat;      // device-path scratch
     DevBuf<int64_t> d_sat2;
     DevBuf<float> d_dinv;
@@ -508,6 +510,7 @@ struct b200_handle {
             if (i8_ok && tc_ok) {
                 s.peaks.alloc(P);
                 CK(cudaMemset(s.peaks.p, 0, P * sizeof(PeakInfo)));
+                s.queue.alloc(P + 1);
             }
             s.gross.alloc(2 * P);
             s.out.alloc(7 * P);
@@ -538,6 +541,7 @@ struct b200_handle {
         if (i8_ok && tc_ok) {
             d_peaks.alloc(G * nwin);
             CK(cudaMemset(d_peaks.p, 0, G * nwin * sizeof(PeakInfo)));
+            d_queue.alloc(G * nwin + 1);
         }
         if (tc_ok) {
             const CUtensorMap m = dinv_map(d_dinv.p, height, width, dpitch(), int(G), M);
@@ -548,22 +552,32 @@ struct b200_handle {
     // the tables and the correlation of nf frames (device memory) on stream s; bstat (the box table
     // beside dinv) serves the exact tensor-core form
     void run_group(const uint8_t *frames, int pitch, int nf, const int32_t *gross, int gross_mode,
-                   uint32_t *sat, int64_t *sat2, float *dinv, int2 *bstat, PeakInfo *peaks, float *offset, float *peak,
-                   float *snr, float *cov, float *surface, cudaStream_t s)
+                   uint32_t *sat, int64_t *sat2, float *dinv, int2 *bstat, PeakInfo *peaks, int *queue, float *offset,
+                   float *peak, float *snr, float *cov, float *surface, cudaStream_t s)
     {
         const int arith = form != B200_FORM_I8 ? form : (bstat && ref_u8) ? B200_FORM_I8 : B200_FORM_FFT32;
         // the tensor-core form's peaks are refined exactly where the reference windows are at hand
-        const bool refine = arith == B200_FORM_TC && peaks && bstat && ref_u8;
+        const bool refine = arith == B200_FORM_TC && peaks && queue && bstat && ref_u8;
         run_tables(frames, pitch, nf, sat, sat2, dinv, s, arith == B200_FORM_I8 || refine ? bstat : nullptr);
         CorrArgs a = corr_args(frames, pitch, nf, gross, gross_mode, sat, dinv, offset, peak, snr, cov, surface);
         a.bstat = bstat;
         a.peaks = refine ? peaks : nullptr;
         run_corr_tail(a, nf, dinv, arith, s);
         if (refine) {
+            CK(cudaMemsetAsync(queue, 0, sizeof(int), s));
             const int64_t threads = int64_t(nf) * nwin * 32;
-            tc_refine_kernel<<<unsigned((threads + 255) / 256), 256, 0, s>>>(a, d_refwin.p, d_sref.p);
+            tc_refine_kernel<<<unsigned((threads + 255) / 256), 256, 0, s>>>(a, d_refwin.p, d_sref.p, queue);
+            const size_t psm = tc_patch_smem(W, M, stat);
+            static bool attr[64] = {};
+            int dev = 0;
+            CK(cudaGetDevice(&dev));
+            if (dev >= 0 && dev < 64 && !attr[dev]) {
+                CK(cudaFuncSetAttribute(tc_patch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+                attr[dev] = true;
+            }
+            tc_patch_kernel<<<unsigned(2 * num_sms()), 256, psm, s>>>(a, d_refwin.p, d_sref.p, queue);
             CK(cudaGetLastError());
-            launches += 1;
+            launches += 2;
         }
         launches += 3;
     }
@@ -1016,7 +1030,7 @@ int b200_correlate(b200_handle *h, const uint8_t *frames, int n, const int32_t *
             CK(cudaEventRecord(s.in, h->copy));
             CK(cudaStreamWaitEvent(h->comp, s.in, 0));
             float *o = s.out.p;
-            h->run_group(s.frames.p, h->fpitch, nf, dg, gross_mode, s.sat.p, s.sat2.p, s.dinv.p, s.bstat.p, s.peaks.p, o, o + 2 * PG,
+            h->run_group(s.frames.p, h->fpitch, nf, dg, gross_mode, s.sat.p, s.sat2.p, s.dinv.p, s.bstat.p, s.peaks.p, s.queue.p, o, o + 2 * PG,
                          o + 3 * PG, o + 4 * PG, nullptr, h->comp);
             CK(cudaMemcpyAsync(s.hout.p, s.out.p, 7 * PG * sizeof(float), cudaMemcpyDeviceToHost, h->comp));
             CK(cudaEventRecord(s.done, h->comp));
@@ -1053,7 +1067,7 @@ static int correlate_device(b200_handle *h, const uint8_t *frames, int n, int pi
             const size_t q0 = size_t(f0) * nwin;
             const int32_t *g = gross_mode == B200_GROSS_FRAME ? gross + 2 * size_t(f0)
                              : gross_mode == B200_GROSS_WINDOW ? gross + 2 * q0 : nullptr;
-            h->run_group(frames + f0 * fstride, pitch, nf, g, gross_mode, h->d_sat.p, h->d_sat2.p, h->d_dinv.p, h->d_bstat.p, h->d_peaks.p,
+            h->run_group(frames + f0 * fstride, pitch, nf, g, gross_mode, h->d_sat.p, h->d_sat2.p, h->d_dinv.p, h->d_bstat.p, h->d_peaks.p, h->d_queue.p,
                          offset + 2 * q0, peak + q0, snr + q0, cov + 3 * q0,
                          surface ? surface + q0 * size_t(h->M) * h->M : nullptr, s);
         }
