@@ -337,6 +337,26 @@ B200_API int b200_tc_i8_selftest(const uint8_t *A, const uint8_t *X, int32_t *D,
 /* The arithmetic of the transforms, B200_FORM_*; B200_EINVAL for an unknown or unbuilt form. */
 B200_API int b200_set_form(b200_handle *h, int form);
 
+/* The device status of a handle's work: waits for `stream` (the caller's, as given to the device
+ * entry points; NULL for the legacy default stream) and the handle's own stream, then *status = 0,
+ * or 3 if a bounded wait inside a tensor-core kernel gave up since the last query (those outputs
+ * are not valid); the flag is cleared. The host entry point b200_correlate checks it itself and
+ * returns B200_ETIMEOUT; callers of the device entry points, which do not synchronize, call this
+ * when they need to know. The reference has no device waits (cxx/cuda.cu:28-40 checks every CUDA
+ * call's status instead). */
+B200_API int b200_status(b200_handle *h, void *stream, int *status);
+
+/* For tests of the error paths, with no GPU fault: the nth device or page-locked allocation from
+ * now fails as an out-of-memory would (B200_ERUNTIME, "framecor: cudaMalloc: out of memory
+ * (injected)"); 0 disables. No counterpart in the reference. */
+B200_API int b200_inject_alloc_failure(int nth);
+
+/* A check of the bounded waits of the tensor-core kernels, with nothing in flight: one thread waits
+ * on an mbarrier that nothing arrives at, with an iteration bound of `polls` and then a clock bound
+ * of limit_ms (at most 1000). B200_ETIMEOUT when both waits gave up, as they must; B200_ERUNTIME
+ * otherwise. The context stays usable. Synchronous on `stream`. No counterpart in the reference. */
+B200_API int b200_wait_selftest(unsigned polls, double limit_ms, void *stream);
+
 /* The grid shape (Correlator.shape, bindings.cpp:139), the FFT size used for the search windows,
  * and the number of kernels this handle has launched (a running count). */
 B200_API int b200_info(const b200_handle *h, int *ny, int *nx, int *fft_size, uint64_t *launches);

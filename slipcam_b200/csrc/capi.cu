@@ -8,6 +8,7 @@
 // device correlates group g, the copy stream brings group g + 1 in and the host stages group g + 2.
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <condition_variable>
 #include <cstdio>
@@ -67,6 +68,18 @@ int fft_size(int L)
     return 0;
 }
 
+// the failure injection of the tests: the n-th device or page-locked allocation from now fails as an
+// out-of-memory would (0: none)
+std::atomic<int> g_fail_alloc{0};
+
+void injected_failure(const char *what)
+{
+    int n = g_fail_alloc.load();
+    while (n > 0 && !g_fail_alloc.compare_exchange_weak(n, n - 1)) {
+    }
+    if (n == 1) fail(B200_ERUNTIME, std::string(what) + ": out of memory (injected)");
+}
+
 template <class T>
 struct DevBuf {
     T *p = nullptr;
@@ -76,6 +89,7 @@ struct DevBuf {
         if (p) cudaFree(p);
         p = nullptr;
         n = count;
+        injected_failure("cudaMalloc");
         CK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
     }
     ~DevBuf()
@@ -91,6 +105,7 @@ struct HostBuf {
     {
         if (p) cudaFreeHost(p);
         p = nullptr;
+        injected_failure("cudaMallocHost");
         CK(cudaMallocHost(&p, std::max<size_t>(count, 1) * sizeof(T)));
     }
     ~HostBuf()
@@ -976,6 +991,7 @@ int b200_correlate(b200_handle *h, const uint8_t *frames, int n, const int32_t *
         if (!frames || !offset || !peak || !snr || !cov) fail(B200_EINVAL, "null input or output");
         CK(cudaSetDevice(h->device));
         h->ensure_slots();
+        CK(cudaMemset(h->d_status.p, 0, sizeof(int)));   // a flag left by an earlier call is not this one's
         const int G = h->group, nwin = h->nwin;
         const size_t frame_bytes = size_t(h->height) * h->width;
         const int ngroups = (n + G - 1) / G;
@@ -1664,6 +1680,43 @@ int b200_profile_read(b200_handle *h, double *kernel_ms, uint64_t *kernel_launch
         if (pairs) *pairs = np;
         h->timed.clear();
     });
+}
+
+int b200_status(b200_handle *h, void *stream, int *status)
+{
+    return guarded(h, [&] {
+        if (!status) fail(B200_EINVAL, "no status output");
+        CK(cudaSetDevice(h->device));
+        CK(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+        CK(cudaStreamSynchronize(h->comp));
+        int st = 0;
+        CK(cudaMemcpy(&st, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (st) CK(cudaMemset(h->d_status.p, 0, sizeof(int)));
+        *status = st;
+    });
+}
+
+int b200_inject_alloc_failure(int nth)
+{
+    if (nth < 0) return B200_EINVAL;
+    g_fail_alloc.store(nth);
+    return B200_OK;
+}
+
+int b200_wait_selftest(unsigned polls, double limit_ms, void *stream)
+{
+    if (polls < 1 || !(limit_ms > 0.0) || limit_ms > 1000.0) return B200_EINVAL;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int *d = nullptr;
+    if (cudaMallocAsync(&d, 2 * sizeof(int), s) != cudaSuccess) return B200_ERUNTIME;
+    wait_selftest_kernel<<<1, 32, 0, s>>>(polls, uint64_t(limit_ms * 1e6), d);
+    int out[2] = {0, 0};
+    const bool ok = cudaGetLastError() == cudaSuccess &&
+                    cudaMemcpyAsync(out, d, sizeof(out), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+                    cudaStreamSynchronize(s) == cudaSuccess;
+    cudaFreeAsync(d, s);
+    if (!ok) return B200_ERUNTIME;
+    return out[0] && out[1] ? B200_ETIMEOUT : B200_ERUNTIME;
 }
 
 int b200_info(const b200_handle *h, int *ny, int *nx, int *fft_size, uint64_t *launches)

@@ -154,7 +154,8 @@ __device__ __forceinline__ bool try_wait(uint32_t addr, uint32_t parity)
 // wait for the phase `parity` of an mbarrier; false if *abort was raised or about two seconds
 // passed (then *abort is raised here). sleep_ns > 0: a waiting role that is not on the critical
 // path sleeps between polls and leaves the issue slots to the others.
-__device__ __forceinline__ bool wait(uint64_t *bar, uint32_t parity, volatile int *abort, unsigned sleep_ns = 0)
+__device__ __forceinline__ bool wait(uint64_t *bar, uint32_t parity, volatile int *abort, unsigned sleep_ns = 0,
+                                     uint64_t limit_ns = 2000000000ull)
 {
     const uint32_t addr = tc::smem_u32(bar);
     if (try_wait(addr, parity)) return true;
@@ -167,7 +168,7 @@ __device__ __forceinline__ bool wait(uint64_t *bar, uint32_t parity, volatile in
             if (*abort) return false;
             const uint64_t t = globaltimer();
             if (!t0) t0 = t;
-            else if (t - t0 > 2000000000ull || it > (1u << 30)) {   // about two seconds
+            else if (t - t0 > limit_ns || it > (1u << 30)) {   // about two seconds by default
                 *abort = 1;
                 return false;
             }
@@ -659,6 +660,23 @@ __global__ void __launch_bounds__(kI8Threads, 1) corr_i8_kernel(I8Args args)
     __syncthreads();
     if (tid == 0 && s_abort && args.status) atomicExch(args.status, 3);
     if (warp == 0) tc::tmem_dealloc(tmem, 512);
+}
+
+// A check of the bounded waits the tensor-core kernels rely on, with nothing in flight on the tensor
+// core: one thread waits on an mbarrier that nothing arrives at, first with the iteration bound of
+// corr_tc_kernel (tc::mbar_wait, `polls` polls), then with the clock bound of corr_i8_kernel
+// (i8::wait, `limit_ns`). out[0] and out[1]: 1 when the wait gave up (as it must), 0 if it returned
+// as completed.
+__global__ void wait_selftest_kernel(uint32_t polls, uint64_t limit_ns, int *out)
+{
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int s_abort;
+    if (threadIdx.x != 0) return;
+    tc::mbar_init(&bar, 1);
+    s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    out[0] = tc::mbar_wait(&bar, 0, polls) ? 0 : 1;
+    out[1] = i8::wait(&bar, 0, &s_abort, 0, limit_ns) ? 0 : 1;
 }
 
 // the reference windows' pixels (nwin x W x W) and their sums, one CTA per window

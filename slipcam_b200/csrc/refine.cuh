@@ -26,7 +26,7 @@ __global__ void __launch_bounds__(256) tc_refine_kernel(CorrArgs a, const uint8_
     const PeakInfo &pi = a.peaks[p];
     const int k = int(p % a.nwin), f = int(p / a.nwin);
     const i8::Pair o = i8::pair(a, k, f);
-    const int W = a.W, M = a.M, L = a.L, n = W * W;
+    const int W = a.W, M = a.M, n = W * W;
     // only pairs the tensor-core kernel found a peak for (the search window inside the frame)
     if (!o.ok || !pi.valid || pi.u < 0 || pi.u >= M || pi.v < 0 || pi.v >= M) return;
     const uint8_t *chip = a.frames + o.f * a.fstride + int64_t(o.sy) * a.pitch + o.sx;
@@ -43,26 +43,22 @@ __global__ void __launch_bounds__(256) tc_refine_kernel(CorrArgs a, const uint8_
         u1 = pu < M - 1 ? 1 : 0;
         v0 = pv > 0 ? -1 : 0;
         v1 = pv < M - 1 ? 1 : 0;
+        // lanes along the columns j (coalesced bytes, the chip rows cached in L1), rows in turn
         int s[3][3] = {};
-        for (int i = lane; i < W; i += 32) {
+        for (int i = 0; i < W; ++i) {
             const uint8_t *rr = ref + size_t(i) * W;
-            for (int du = u0; du <= u1; ++du) {
-                // chip row pu + du + i, columns pv + v0 .. pv + v1 + W - 1 (all inside [0, L))
-                const uint8_t *cr = chip + int64_t(pu + du + i) * a.pitch + pv;
-                int sm = 0, s0 = 0, sp = 0;
-                uint32_t bm = v0 < 0 ? __ldg(cr - 1) : 0u, b0 = __ldg(cr);
-                for (int j = 0; j < W; ++j) {
-                    const uint32_t x = __ldg(rr + j);
-                    const uint32_t bp = (v1 > 0 || j + 1 < W) && pv + j + 1 < L ? __ldg(cr + j + 1) : 0u;
-                    sm += int(x * bm);
-                    s0 += int(x * b0);
-                    sp += int(x * bp);
-                    bm = b0;
-                    b0 = bp;
+            for (int j = lane; j < W; j += 32) {
+                const uint32_t x = __ldg(rr + j);
+#pragma unroll
+                for (int du = -1; du <= 1; ++du) {
+                    if (du < u0 || du > u1) continue;
+                    // chip row pu + du + i, columns pv + v0 + j .. pv + v1 + j (inside [0, L))
+                    const uint8_t *cr = chip + int64_t(pu + du + i) * a.pitch + pv + j;
+                    const uint32_t bm = v0 < 0 ? __ldg(cr - 1) : 0u, b0 = __ldg(cr), bp = v1 > 0 ? __ldg(cr + 1) : 0u;
+                    s[du + 1][0] += int(x * bm);
+                    s[du + 1][1] += int(x * b0);
+                    s[du + 1][2] += int(x * bp);
                 }
-                s[du + 1][0] += sm;
-                s[du + 1][1] += s0;
-                s[du + 1][2] += sp;
             }
         }
 #pragma unroll
@@ -153,9 +149,9 @@ __global__ void __launch_bounds__(256) tc_patch_kernel(CorrArgs a, const uint8_t
         for (int idx = warp; idx < np; idx += 8) {
             const int du = idx / pw, dv = idx % pw;
             int acc = 0;
-            for (int i = lane; i < W; i += 32) {
+            for (int i = 0; i < W; ++i) {   // lanes along the columns: conflict-free shared memory
                 const unsigned char *rr = sref_w + i * W, *cr = schip + (du + i) * cols + dv;
-                for (int j = 0; j < W; ++j) acc += int(uint32_t(rr[j]) * uint32_t(cr[j]));
+                for (int j = lane; j < W; j += 32) acc += int(uint32_t(rr[j]) * uint32_t(cr[j]));
             }
             for (int d = 16; d > 0; d >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, d);
             const int u = i0 + du, v = j0 + dv;

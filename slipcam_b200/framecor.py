@@ -132,6 +132,17 @@ class Correlator:
             raise ValueError(f'framecor: unknown form {form}')
         _lib.raise_for(_lib.lib().b200_set_form(self._h, code), self._h)
 
+    def check(self, stream=None):
+        """After device-path calls (CUDA tensors, no host synchronization): wait for them and raise
+        RuntimeError if a bounded wait inside a tensor-core kernel gave up since the last check (their
+        outputs are not valid). The host-array path checks by itself."""
+        import torch
+        st = ctypes.c_int()
+        s = (stream if stream is not None else torch.cuda.current_stream()).cuda_stream
+        _lib.raise_for(_lib.lib().b200_status(self._h, s, ctypes.byref(st)), self._h)
+        if st.value:
+            raise RuntimeError('framecor: a tensor-core completion wait gave up; the outputs are not valid')
+
     def info(self):
         """(ny, nx, fft_size, kernel launches so far)"""
         ny, nx, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
