@@ -580,16 +580,21 @@ struct b200_handle {
         run_corr_tail(a, nf, dinv, arith, s);
         if (refine) {
             CK(cudaMemsetAsync(queue, 0, sizeof(int), s));
-            const int64_t threads = int64_t(nf) * nwin * 32;
-            tc_refine_kernel<<<unsigned((threads + 255) / 256), 256, 0, s>>>(a, d_refwin.p, d_sref.p, queue);
-            const size_t psm = tc_patch_smem(W, M, stat);
             static bool attr[64] = {};
             int dev = 0;
             CK(cudaGetDevice(&dev));
             if (dev >= 0 && dev < 64 && !attr[dev]) {
                 CK(cudaFuncSetAttribute(tc_patch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+                CK(cudaFuncSetAttribute(tc_refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
                 attr[dev] = true;
             }
+            // one warp per pair, as many warps per CTA as 96 KB of their tiles hold (at most 8)
+            const size_t wsm = refine_warp_smem(W);
+            const int wpc = int(std::clamp<size_t>(size_t(96 * 1024) / wsm, 1, 8));
+            const int64_t pairs = int64_t(nf) * nwin;
+            tc_refine_kernel<<<unsigned((pairs + wpc - 1) / wpc), 32 * wpc, size_t(wpc) * wsm, s>>>(a, d_refwin.p, d_sref.p,
+                                                                                                   queue);
+            const size_t psm = tc_patch_smem(W, M, stat);
             tc_patch_kernel<<<unsigned(2 * num_sms()), 256, psm, s>>>(a, d_refwin.p, d_sref.p, queue);
             CK(cudaGetLastError());
             launches += 2;

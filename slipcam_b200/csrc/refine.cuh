@@ -7,20 +7,88 @@
 // When an exact neighbour is larger than the peak (the FP16 argmax fell on the wrong side of a tie
 // between adjacent shifts), the peak climbs to it and the SNR patch around the new peak is summed
 // exactly; so is the patch of windows up to 32 px, whose small surfaces weigh the FP16 errors more
-// in the SNR. One warp per pair, the reference rows shared between the lanes; the pairs whose patch
-// is summed exactly are queued for tc_patch_kernel, a CTA each.
+// in the SNR. One warp per pair, its reference window and chip region staged in shared memory and
+// summed with dp4a; the pairs whose patch is summed exactly are queued for tc_patch_kernel, a CTA
+// each.
 #pragma once
 
 #include "corr_i8.cuh"
 
 namespace b200 {
 
+// the bytes of a reference row held in shared memory, padded with zeros to whole words
+__host__ __device__ inline int refine_rp(int W) { return (W + 3) & ~3; }
+// the bytes of a staged frame-region row: whole words and one more word for the shifted reads
+__host__ __device__ inline int refine_tp(int nc) { return ((nc + 3) & ~3) + 4; }
+
+// the shared memory of one refinement warp: the reference window and the chip region of the 3 x 3
+__host__ __device__ inline size_t refine_warp_smem(int W)
+{
+    return (size_t(W) * refine_rp(W) + size_t(W + 2) * refine_tp(W + 2) + 15) & ~size_t(15);
+}
+
+// the shared memory tc_patch_kernel needs: the reference window and the chip region of the patch
+__host__ __device__ inline size_t tc_patch_smem(int W, int M, int stat)
+{
+    const int n = stat < M ? stat : M;
+    return size_t(W) * refine_rp(W) + size_t(n + W - 1) * refine_tp(n + W - 1);
+}
+
 #ifdef __CUDACC__
 
+// the reference window (W x W bytes at ref) into dst, rows of rp bytes zero-padded
+__device__ __forceinline__ void stage_ref(unsigned char *dst, const uint8_t *ref, int W, int t, int nt)
+{
+    const int rp = refine_rp(W);
+    if ((W & 3) == 0 && (reinterpret_cast<uintptr_t>(ref) & 3) == 0) {
+        const uint32_t *s = reinterpret_cast<const uint32_t *>(ref);
+        uint32_t *d = reinterpret_cast<uint32_t *>(dst);
+        for (int e = t; e < W * W / 4; e += nt) d[e] = __ldg(s + e);
+    } else {
+        for (int e = t; e < W * rp; e += nt) {
+            const int i = e / rp, j = e - i * rp;
+            dst[e] = j < W ? __ldg(ref + i * W + j) : 0;
+        }
+    }
+}
+
+// nr rows of nc bytes of the frame from src (row pitch `pitch`) into dst, rows of refine_tp(nc)
+// bytes; whole words when the frame rows start on 4-byte boundaries (every aligned word read holds
+// a byte of the region, so no read leaves the region's rows)
+__device__ __forceinline__ void stage_region(unsigned char *dst, const uint8_t *src, int64_t pitch, bool words, int nr,
+                                             int nc, int t, int nt)
+{
+    const int tp = refine_tp(nc), wpr = tp / 4;
+    if (words) {
+        uint32_t *d = reinterpret_cast<uint32_t *>(dst);
+        for (int e = t; e < nr * wpr; e += nt) {
+            const int r = e / wpr, w = e - r * wpr;
+            uint32_t v = 0;
+            if (4 * w < nc) {
+                const uintptr_t base = reinterpret_cast<uintptr_t>(src + int64_t(r) * pitch) + 4 * w;
+                const uint32_t *al = reinterpret_cast<const uint32_t *>(base & ~uintptr_t(3));
+                const int sh = int(base & 3);
+                const uint32_t lo = __ldg(al), hi = (sh != 0 && 4 * w + 4 - sh < nc) ? __ldg(al + 1) : 0u;
+                v = __funnelshift_r(lo, hi, 8 * sh);
+            }
+            d[e] = v;
+        }
+    } else {
+        for (int e = t; e < nr * tp; e += nt) {
+            const int r = e / tp, c = e - r * tp;
+            dst[e] = c < nc ? __ldg(src + int64_t(r) * pitch + c) : 0;
+        }
+    }
+}
+
+// the exact refinement: one warp per pair, its reference window and 3 x 3 chip region staged in
+// the warp's part of the shared memory, the nine sums taken with dp4a (four uint8 products a
+// step), the lanes along the words of the reference rows
 __global__ void __launch_bounds__(256) tc_refine_kernel(CorrArgs a, const uint8_t *refwin, const int *sref,
                                                         int *queue)
 {
-    const int lane = threadIdx.x & 31;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t p = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;   // the pair (its output index)
     if (p >= int64_t(a.nwin) * a.nf) return;
     const PeakInfo &pi = a.peaks[p];
@@ -29,11 +97,16 @@ __global__ void __launch_bounds__(256) tc_refine_kernel(CorrArgs a, const uint8_
     const int W = a.W, M = a.M, n = W * W;
     // only pairs the tensor-core kernel found a peak for (the search window inside the frame)
     if (!o.ok || !pi.valid || pi.u < 0 || pi.u >= M || pi.v < 0 || pi.v >= M) return;
+    unsigned char *sref_w = smem + size_t(warp) * refine_warp_smem(W);
+    unsigned char *tile = sref_w + size_t(W) * refine_rp(W);
     const uint8_t *chip = a.frames + o.f * a.fstride + int64_t(o.sy) * a.pitch + o.sx;
+    const bool words = ((a.pitch | int(a.fstride & 3) | int(reinterpret_cast<uintptr_t>(a.frames) & 3)) & 3) == 0;
     const uint8_t *ref = refwin + size_t(k) * W * W;
     const float scale = float(1.0 / (double(n) * double(a.norm[k])));
     const int2 *bt0 = a.bstat + size_t(o.f) * a.dinv_fstride + size_t(o.sy) * a.dpitch + o.sx;
     const int sr = sref[k];
+    const int wpr = refine_rp(W) / 4;
+    stage_ref(sref_w, ref, W, lane, 32);
     int pu = pi.u, pv = pi.v;
     float fit[9];
     int u0 = 0, u1 = 0, v0 = 0, v1 = 0;
@@ -43,27 +116,27 @@ __global__ void __launch_bounds__(256) tc_refine_kernel(CorrArgs a, const uint8_
         u1 = pu < M - 1 ? 1 : 0;
         v0 = pv > 0 ? -1 : 0;
         v1 = pv < M - 1 ? 1 : 0;
-        // lanes along the columns j (coalesced bytes, the chip rows cached in L1), rows in turn
-        int s[3][3] = {};
-        for (int i = 0; i < W; ++i) {
-            const uint8_t *rr = ref + size_t(i) * W;
-            for (int j = lane; j < W; j += 32) {
-                const uint32_t x = __ldg(rr + j);
+        const int nr = W + u1 - u0, nc = W + v1 - v0, tp = refine_tp(nc);
+        __syncwarp();
+        stage_region(tile, chip + int64_t(pu + u0) * a.pitch + pv + v0, a.pitch, words, nr, nc, lane, 32);
+        __syncwarp();
+        uint32_t s[3][3] = {};
+        for (int it = lane; it < W * wpr; it += 32) {
+            const int i = it / wpr, w = it - i * wpr;
+            const uint32_t rw = *reinterpret_cast<const uint32_t *>(sref_w + i * refine_rp(W) + 4 * w);
 #pragma unroll
-                for (int du = -1; du <= 1; ++du) {
-                    if (du < u0 || du > u1) continue;
-                    // chip row pu + du + i, columns pv + v0 + j .. pv + v1 + j (inside [0, L))
-                    const uint8_t *cr = chip + int64_t(pu + du + i) * a.pitch + pv + j;
-                    const uint32_t bm = v0 < 0 ? __ldg(cr - 1) : 0u, b0 = __ldg(cr), bp = v1 > 0 ? __ldg(cr + 1) : 0u;
-                    s[du + 1][0] += int(x * bm);
-                    s[du + 1][1] += int(x * b0);
-                    s[du + 1][2] += int(x * bp);
-                }
+            for (int du = 0; du < 3; ++du) {
+                if (du > u1 - u0) continue;
+                const uint32_t *row = reinterpret_cast<const uint32_t *>(tile + (i + du) * tp) + w;
+                const uint32_t lo = row[0], hi = row[1];
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    if (d <= v1 - v0) s[du][d] = __dp4a(rw, d ? __funnelshift_r(lo, hi, 8 * d) : lo, s[du][d]);
             }
         }
 #pragma unroll
         for (int t = 0; t < 9; ++t)
-            for (int d = 16; d > 0; d >>= 1) s[t / 3][t % 3] += __shfl_xor_sync(0xffffffffu, s[t / 3][t % 3], d);
+            for (int dd = 16; dd > 0; dd >>= 1) s[t / 3][t % 3] += __shfl_xor_sync(0xffffffffu, s[t / 3][t % 3], dd);
         // the exact values, and the best of the 3 x 3 (the reference's rule: the larger, the first in
         // raster order if equal); every lane computes the same
         float best = -2.0f;
@@ -72,7 +145,7 @@ __global__ void __launch_bounds__(256) tc_refine_kernel(CorrArgs a, const uint8_
             for (int dv = v0; dv <= v1; ++dv) {
                 const int t = (du + 1) * 3 + dv + 1;
                 const int2 st = __ldg(bt0 + int64_t(pu + du) * a.dpitch + pv + dv);
-                fit[t] = i8::rho(uint32_t(s[du + 1][dv + 1]), st, n, sr, scale);
+                fit[t] = i8::rho(s[du - u0][dv - v0], st, n, sr, scale);
                 const int at = (pu + du) * M + pv + dv;
                 if (fit[t] > best || (fit[t] == best && at < bat)) {
                     best = fit[t];
@@ -110,23 +183,19 @@ __global__ void __launch_bounds__(256) tc_refine_kernel(CorrArgs a, const uint8_
                  a.cov);
 }
 
-// the shared memory tc_patch_kernel needs: the reference window and the chip region of the patch
-inline size_t tc_patch_smem(int W, int M, int stat)
-{
-    const int n = stat < M ? stat : M;
-    return size_t(W) * W + size_t(n + W - 1) * (n + W - 1);
-}
-
-// the SNR patch of each queued pair summed exactly (one CTA per pair: the reference window and the
-// chip region in shared memory, a warp per patch position), then the pair's outputs
+// the SNR patch of each queued pair summed exactly: one CTA per pair, the reference window and the
+// patch's chip region in shared memory, a thread per patch position (dp4a over the reference rows'
+// words), then the pair's outputs
 __global__ void __launch_bounds__(256) tc_patch_kernel(CorrArgs a, const uint8_t *refwin, const int *sref,
                                                        const int *queue)
 {
-    extern __shared__ unsigned char sm[];
+    extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double s_sum[8];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int W = a.W, M = a.M, n = W * W;
+    const int W = a.W, M = a.M, n = W * W, rp = refine_rp(W), wpr = rp / 4;
+    const bool words = ((a.pitch | int(a.fstride & 3) | int(reinterpret_cast<uintptr_t>(a.frames) & 3)) & 3) == 0;
     const int count = queue[0];
+    unsigned char *sref_w = smem, *tile = smem + size_t(W) * rp;
     for (int t = blockIdx.x; t < count; t += gridDim.x) {
         const int p = queue[1 + t];
         const PeakInfo &pi = a.peaks[p];
@@ -135,29 +204,28 @@ __global__ void __launch_bounds__(256) tc_patch_kernel(CorrArgs a, const uint8_t
         const int pu = pi.u, pv = pi.v;
         int i0, i1, j0, j1;
         snr_patch(M, a.stat, pu, pv, i0, i1, j0, j1);
-        const int rows = i1 - i0 + W - 1, cols = j1 - j0 + W - 1;
-        unsigned char *sref_w = sm, *schip = sm + size_t(W) * W;
-        const uint8_t *ref = refwin + size_t(k) * W * W;
-        for (int e = tid; e < W * W; e += 256) sref_w[e] = __ldg(ref + e);
-        const uint8_t *chip = a.frames + o.f * a.fstride + int64_t(o.sy + i0) * a.pitch + o.sx + j0;
-        for (int e = tid; e < rows * cols; e += 256) schip[e] = __ldg(chip + int64_t(e / cols) * a.pitch + e % cols);
+        const int pw = j1 - j0, np = (i1 - i0) * pw;
+        const int nr = i1 - i0 + W - 1, nc = pw + W - 1, tp = refine_tp(nc);
+        stage_ref(sref_w, refwin + size_t(k) * W * W, W, tid, 256);
+        stage_region(tile, a.frames + o.f * a.fstride + int64_t(o.sy + i0) * a.pitch + o.sx + j0, a.pitch, words, nr, nc,
+                     tid, 256);
         __syncthreads();
         const float scale = float(1.0 / (double(n) * double(a.norm[k])));
         const int2 *bt0 = a.bstat + size_t(o.f) * a.dinv_fstride + size_t(o.sy) * a.dpitch + o.sx;
-        const int pw = j1 - j0, np = (i1 - i0) * pw;
         double sum = 0.0;
-        for (int idx = warp; idx < np; idx += 8) {
-            const int du = idx / pw, dv = idx % pw;
-            int acc = 0;
-            for (int i = 0; i < W; ++i) {   // lanes along the columns: conflict-free shared memory
-                const unsigned char *rr = sref_w + i * W, *cr = schip + (du + i) * cols + dv;
-                for (int j = lane; j < W; j += 32) acc += int(uint32_t(rr[j]) * uint32_t(cr[j]));
+        for (int q = tid; q < np; q += 256) {
+            const int du = q / pw, dv = q - du * pw;
+            const int sh = 8 * (dv & 3);
+            uint32_t acc = 0;
+            for (int i = 0; i < W; ++i) {
+                const uint32_t *rr = reinterpret_cast<const uint32_t *>(sref_w + i * rp);
+                const uint32_t *cr = reinterpret_cast<const uint32_t *>(tile + (du + i) * tp + (dv & ~3));
+                for (int w = 0; w < wpr; ++w) acc = __dp4a(rr[w], __funnelshift_r(cr[w], cr[w + 1], sh), acc);
             }
-            for (int d = 16; d > 0; d >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, d);
-            const int u = i0 + du, v = j0 + dv;
-            const float x = i8::rho(uint32_t(acc), __ldg(bt0 + int64_t(u) * a.dpitch + v), n, sref[k], scale);
+            const float x = i8::rho(acc, __ldg(bt0 + int64_t(i0 + du) * a.dpitch + j0 + dv), n, sref[k], scale);
             sum += double(x) * double(x);
         }
+        for (int d = 16; d > 0; d >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, d);
         if (lane == 0) s_sum[warp] = sum;
         __syncthreads();
         if (tid == 0) {

@@ -69,6 +69,15 @@ def case(name):
         rng = np.random.default_rng(7)
         down, across = window_grid(h, w, W, R, skip, margin)
         gross = rng.integers(-8, 9, size=(2, len(down), len(across), 2)).astype(np.int32)
+    elif name in C3:              # a 2-frame slice of the mixed-grid 720p workload (10 % flat, 5 %
+        # saturated, an 8 px striped box), one of its three grids, per-window gross U[-20, 20]
+        h, w, skip, margin = 720, 1280, 16, 0
+        W, R = C3[name]
+        v, _ = synth.mixed(n=3, h=h, w=w)
+        ref, frames = v[0], v[1:]
+        rng = np.random.default_rng(W)
+        down, across = window_grid(h, w, W, R, skip, margin)
+        gross = rng.integers(-20, 21, size=(2, len(down), len(across), 2)).astype(np.int32)
     else:
         raise KeyError(name)
     down, across = window_grid(h, w, W, R, skip, margin)
@@ -77,7 +86,10 @@ def case(name):
                 frames=np.ascontiguousarray(frames), gross=gross)
 
 
-NAMES = ['shifts', 'gross', 'window_gross', 'invalid', 'small', 'hd', 'wide', 'big', 'mixed']
+C3 = {'c3_w32': (32, 16), 'c3_w64': (64, 48), 'c3_w128': (128, 64)}
+NAMES = ['shifts', 'gross', 'window_gross', 'invalid', 'small', 'hd', 'wide', 'big', 'mixed', *C3]
+# the large cases, checked against the FP64 oracle on a sub-grid (every a-th row, b-th column)
+SUBGRID = {'hd': (7, 9), 'c3_w32': (7, 9), 'c3_w64': (7, 9), 'c3_w128': (5, 9)}
 
 
 def digest(c):

@@ -8,7 +8,7 @@ import pytest
 
 import cases
 
-SUBGRID = {'hd': (7, 9)}   # the oracle sums directly: a sub-grid of the 720p windows
+SUBGRID = cases.SUBGRID   # the oracle sums directly: a sub-grid of the 720p windows
 
 
 def load(name):

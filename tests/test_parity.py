@@ -37,6 +37,12 @@ def b200(c, gross=None, frames=None):
     return cor, cor.correlate(c['frames'] if frames is None else frames, gross=c['gross'] if gross is None else gross)
 
 
+def subgrid(name):
+    """the frames, rows and columns of windows a case is checked on against the FP64 oracle"""
+    a, b = cases.SUBGRID.get(name, (1, 1))
+    return (slice(None), slice(None, None, a), slice(None, None, b))
+
+
 def sub(c, sl):
     """The windows and the gross offsets of the sub-grid sl (frames, rows, columns) of case c."""
     g = oracle.expand_gross(c['gross'], len(c['frames']), len(c['down']), len(c['across']))
@@ -112,15 +118,13 @@ def test_golden(name):
     assert np.abs(r['snr'][ok] / g['snr'][ok] - 1).max() < 1e-2
 
 
-@pytest.mark.parametrize('name', ['shifts', 'gross', 'window_gross', 'small', 'hd', 'wide', 'mixed'])
+@pytest.mark.parametrize('name', ['shifts', 'gross', 'window_gross', 'small', 'hd', 'wide', 'mixed', *cases.C3])
 def test_fp64_oracle(name):
     """b200 against the FP64 direct-correlation oracle: the 0.01 px gate."""
     c = cases.case(name)
     _, r = b200(c)
-    down, across, gross = c['down'], c['across'], c['gross']
-    sl = (slice(None), slice(None, None, 7), slice(None, None, 9)) if name == 'hd' else (slice(None),) * 3
-    if name == 'hd':
-        down, across = down[::7], across[::9]
+    sl = subgrid(name)
+    down, across, gross = c['down'][sl[1]], c['across'][sl[2]], c['gross']
     o = oracle.correlate(c['height'], c['width'], down, across, c['reference'], c['frames'],
                          gross if gross is None or gross.ndim == 2 else gross[sl], window=c['window'],
                          search=c['search'], stat_size=c['stat_size'], mode='f64')
@@ -223,7 +227,7 @@ def test_hd_recovers_motion():
 # the peak value and the covariance are the exact form's; the SNR keeps the FP16 values of the rest
 # of its patch. The gates are the FP32 form's, on every case: offsets within 0.01 px, SNR within
 # 1e-3 relative of the FP64 oracle, integer peaks identical except near-ties of the FP16 surface.
-TC_CASES = ['shifts', 'gross', 'window_gross', 'invalid', 'small', 'hd', 'mixed']
+TC_CASES = ['shifts', 'gross', 'window_gross', 'invalid', 'small', 'hd', 'mixed', 'c3_w32', 'c3_w64']
 TC_NEAR_TIE = 2e-3   # a near-tie for the FP16 form: within a few times its surface error (3e-4)
 
 
@@ -235,10 +239,8 @@ def test_tc_fp64_oracle(name):
     cor.set_form('tc')
     cor.set_reference(c['reference'])
     r = cor.correlate(c['frames'], gross=c['gross'])
-    down, across, gross = c['down'], c['across'], c['gross']
-    sl = (slice(None), slice(None, None, 7), slice(None, None, 9)) if name == 'hd' else (slice(None),) * 3
-    if name == 'hd':
-        down, across = down[::7], across[::9]
+    sl = subgrid(name)
+    down, across, gross = c['down'][sl[1]], c['across'][sl[2]], c['gross']
     o = oracle.correlate(c['height'], c['width'], down, across, c['reference'], c['frames'],
                          gross if gross is None or gross.ndim == 2 else gross[sl], window=c['window'],
                          search=c['search'], stat_size=c['stat_size'], mode='f64')
