@@ -76,10 +76,9 @@ def near_tie_ok(c, mism, out, ref_out, tol, sl=(slice(None),) * 3):
 
 
 def tie_count(c, tol=NEAR_TIE, sl=(slice(None),) * 3):
-    """The pairs whose FP64 surface holds a second integer peak, outside the maximum's 3 x 3, within
-    tol of the maximum: the only pairs whose integer peak rounding may decide. 'mixed' (flat,
-    saturated and 8 px striped regions) has 182 such pairs of 456, all exact ties; the other cases
-    have none."""
+    """The pairs whose FP64 surface holds another shift within tol of its maximum: the only pairs
+    whose integer peak rounding may decide. 'mixed' (flat, saturated and 8 px striped regions) has
+    182 of 456 (exact ties); the other small cases have none."""
     down, across, gross = sub(c, sl)
     o = oracle.correlate(c['height'], c['width'], down, across, c['reference'], c['frames'], gross,
                          window=c['window'], search=c['search'], stat_size=c['stat_size'], mode='f64', surfaces=True)
@@ -88,11 +87,10 @@ def tie_count(c, tol=NEAR_TIE, sl=(slice(None),) * 3):
     valid = np.isfinite(o['offsets'][..., 0]).reshape(-1)
     n = 0
     for p in np.flatnonzero(valid):
-        f = flat[p]
-        u, v = divmod(int(np.argmax(f)), M)
-        g = f.reshape(M, M).copy()
-        g[max(u - 1, 0):u + 2, max(v - 1, 0):v + 2] = -np.inf
-        n += int(f.max() - g.max() <= tol)
+        f = flat[p].copy()
+        top = f.max()
+        f[int(np.argmax(f))] = -np.inf
+        n += int(top - f.max() <= tol)
     return n
 
 
@@ -108,7 +106,7 @@ def test_golden(name):
     assert np.all(r['snr'][~valid] == 0) and np.all(r['peak'][~valid] == 0)
     assert np.all(r['cov'][~valid] == np.array([99, 99, 0], np.float32))
     d = np.abs(a - b).max(-1)
-    mism = valid & (d > 0.5)
+    mism = valid & (d > 0.1)
     if mism.any():   # every differing integer peak is a verified near-tie, and there are no more than ties
         assert mism.sum() <= tie_count(c), f'{mism.sum()} integer peaks differ'
         assert near_tie_ok(c, mism, r, g, NEAR_TIE)
@@ -132,7 +130,7 @@ def test_fp64_oracle(name):
     assert np.array_equal(np.isnan(o['offsets']), np.isnan(b['offsets']))
     valid = np.isfinite(o['offsets'][..., 0])
     d = np.abs(o['offsets64'] - b['offsets']).max(-1)
-    mism = valid & (d > 0.5)
+    mism = valid & (d > 0.1)
     if mism.any():   # per-frame and per-window gross alike
         assert mism.sum() <= tie_count(c, sl=sl)
         assert near_tie_ok(c, mism, b, o, NEAR_TIE, sl)
@@ -249,7 +247,7 @@ def test_tc_fp64_oracle(name):
     valid = np.isfinite(o['offsets'][..., 0])
     assert np.all(b['cov'][~valid] == np.array([99, 99, 0], np.float32))
     d = np.abs(o['offsets64'] - b['offsets']).max(-1)
-    mism = valid & (d > 0.5)
+    mism = valid & (d > 0.1)
     if mism.any():   # each one a near-tie within the FP16 surface error
         assert mism.sum() <= tie_count(c, TC_NEAR_TIE, sl)
         assert near_tie_ok(c, mism, b, o, TC_NEAR_TIE, sl)
