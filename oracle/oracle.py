@@ -267,11 +267,14 @@ def mask_from_maps(edge, sd, edge_percentile=90, max_std=1.5, dilate=4):
     """
     TEST INFRASTRUCTURE. The rest of auto_slip.text_mask (auto_slip.py:92-94) from the float32 edge
     magnitude and steadiness maps: pixels above numpy.percentile(edge, edge_percentile) and below
-    max_std, dilated `dilate` times by the 3 x 3 cross, then every background region that does not
-    touch the border (4-connected) filled.
+    max_std, dilated `dilate` times by the 3 x 3 cross (dilate < 1: until nothing changes, as
+    scipy.ndimage.binary_dilation does), then every background region that does not touch the border
+    (4-connected) filled.
     """
     from scipy import ndimage
     m = (edge > np.percentile(edge, edge_percentile)) & (sd < max_std)
+    if dilate < 1:   # scipy repeats the dilation until nothing changes: the whole frame if any pixel is set
+        m = np.ones_like(m) if m.any() else m
     for _ in range(dilate):
         g = m.copy()
         g[1:] |= m[:-1]

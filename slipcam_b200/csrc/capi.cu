@@ -480,7 +480,10 @@ struct b200_handle {
     DevBuf<float> d_coarse;      // coarse tracking: one frame's surfaces and four outputs
     DevBuf<double> d_cpeaks;     // coarse tracking: one frame's peaks
     cudaEvent_t coarse_ev[6] = {};  // coarse tracking: tables ready (2), tables consumed (2), call start, end
-    bool coarse_l2 = false;      // the handle's stream keeps the reference spectra in L2
+    bool coarse_l2 = false;      // the persisting L2 carve-out for the reference spectra is set up
+    cudaAccessPolicyWindow l2win{};   // the window coarse tracking puts on the handle's stream per call
+    size_t l2_limit_prev = 0;    // the device's persisting L2 limit before this handle raised it
+    bool l2_raised = false;
     bool tc_ok = false;          // the geometry fits the tensor-core kernel
     bool i8_ok = false;          // the geometry fits the exact tensor-core kernel
     I8Geo i8g{};                 // its layout
@@ -501,6 +504,7 @@ struct b200_handle {
         }
         for (cudaEvent_t e : coarse_ev)
             if (e) cudaEventDestroy(e);
+        if (l2_raised) cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, l2_limit_prev);   // as it was
         if (comp) cudaStreamDestroy(comp);
         if (copy) cudaStreamDestroy(copy);
     }
@@ -1396,7 +1400,7 @@ size_t b200_text_mask_scratch_bytes(int height, int width)
 int b200_text_mask_device(const float *edge, const float *sd, int height, int width, double edge_percentile, float max_std,
                           int dilate, uint8_t *mask, void *scratch, size_t scratch_bytes, void *stream)
 {
-    if (height <= 0 || width <= 0 || dilate < 0 || !edge || !sd || !mask || !scratch) return B200_EINVAL;
+    if (height <= 0 || width <= 0 || !edge || !sd || !mask || !scratch) return B200_EINVAL;
     const int64_t n = int64_t(height) * width;
     const int wpr = (width + 31) / 32;
     const size_t tile = size_t(2) * (kDilateRows + 2 * kDilateStep) * wpr * 4;   // the dilation's shared memory
@@ -1408,6 +1412,12 @@ int b200_text_mask_device(const float *edge, const float *sd, int height, int wi
     uint32_t *m = reinterpret_cast<uint32_t *>(static_cast<char *>(scratch) + kSelectScratch), *o = m + int64_t(height) * wpr;
     text_seed_bits_kernel<<<unsigned((int64_t(height) * wpr * 32 + 255) / 256), 256, 0, s>>>(edge, sd, height, width, wpr,
                                                                                              thr, max_std, m);
+    if (dilate < 1) {   // until nothing changes (scipy's iterations < 1): every pixel if any is set
+        const int64_t words = int64_t(height) * wpr;
+        if (cudaMemsetAsync(o, 0, sizeof(uint32_t), s) != cudaSuccess) return B200_ERUNTIME;
+        any_bits_kernel<<<unsigned(std::min<int64_t>((words + 255) / 256, 1184)), 256, 0, s>>>(m, words, o);
+        all_bits_kernel<<<unsigned((words + 255) / 256), 256, 0, s>>>(m, height, width, wpr, o);
+    }
     for (int done = 0; done < dilate; done += kDilateStep) {
         const int steps = std::min(kDilateStep, dilate - done);
         const size_t bytes = size_t(2) * (kDilateRows + 2 * steps) * wpr * 4;
@@ -1483,24 +1493,29 @@ int b200_coarse_track_device(b200_handle *h, const uint8_t *frames, int n, int p
         // caller's next: there the grid's reference spectra persist in L2 (every frame reads them;
         // the next group's tables, written beside the chain, would otherwise evict them)
         cudaStream_t s = h->comp;
-        if (!h->coarse_l2) {
+        if (!h->coarse_l2) {   // the carve-out once per handle (the previous limit comes back at destroy)
             cudaDeviceProp prop{};
             CK(cudaGetDeviceProperties(&prop, h->device));
             const size_t want = nwin * size_t(h->N / 2 + 1) * h->N * sizeof(float2);
             const size_t carve = std::min<size_t>(want, size_t(prop.persistingL2CacheMaxSize));
             size_t cur = 0;
             CK(cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize));
-            if (carve > cur) CK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, carve));
-            cudaStreamAttrValue v{};
-            v.accessPolicyWindow.base_ptr = h->d_spec.p;
-            v.accessPolicyWindow.num_bytes = std::min<size_t>(want, size_t(prop.accessPolicyMaxWindowSize));
-            v.accessPolicyWindow.hitRatio = carve >= v.accessPolicyWindow.num_bytes
-                                                ? 1.0f
-                                                : float(double(carve) / double(v.accessPolicyWindow.num_bytes));
-            v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
-            v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
-            CK(cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &v));
+            if (carve > cur) {
+                CK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, carve));
+                h->l2_limit_prev = cur;
+                h->l2_raised = true;
+            }
+            h->l2win.base_ptr = h->d_spec.p;
+            h->l2win.num_bytes = std::min<size_t>(want, size_t(prop.accessPolicyMaxWindowSize));
+            h->l2win.hitRatio = carve >= h->l2win.num_bytes ? 1.0f : float(double(carve) / double(h->l2win.num_bytes));
+            h->l2win.hitProp = cudaAccessPropertyPersisting;
+            h->l2win.missProp = cudaAccessPropertyStreaming;
             h->coarse_l2 = true;
+        }
+        {   // the window covers this call's chain only: the handle's stream serves other calls too
+            cudaStreamAttrValue v{};
+            v.accessPolicyWindow = h->l2win;
+            CK(cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &v));
         }
         CK(cudaEventRecord(h->coarse_ev[4], caller));
         CK(cudaStreamWaitEvent(s, h->coarse_ev[4], 0));
@@ -1537,6 +1552,9 @@ int b200_coarse_track_device(b200_handle *h, const uint8_t *frames, int n, int p
             h->launches += 3;
         };
         CK(cudaStreamWaitEvent(side, start, 0));   // the frames and the state are written on the caller's stream
+        // and the previous call's chain, which may still read both table sets, is done with them (a
+        // caller that changes streams between calls orders nothing by itself)
+        CK(cudaStreamWaitEvent(side, h->coarse_ev[5], 0));
         tables(0);
         for (int g = 0; g < groups; ++g) {
             if (g + 1 < groups) tables(g + 1);
@@ -1566,6 +1584,9 @@ int b200_coarse_track_device(b200_handle *h, const uint8_t *frames, int n, int p
         }
         CK(cudaEventRecord(h->coarse_ev[5], s));   // the caller's stream continues after the chain
         CK(cudaStreamWaitEvent(caller, h->coarse_ev[5], 0));
+        cudaStreamAttrValue none{};   // later launches on the handle's stream carry no window
+        none.accessPolicyWindow.num_bytes = 0;
+        CK(cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &none));
     });
 }
 

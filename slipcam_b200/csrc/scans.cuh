@@ -371,6 +371,26 @@ __device__ __forceinline__ uint32_t row_bits(int c, int w)   // the bits of word
     return rem >= 32 ? 0xFFFFFFFFu : ((1u << rem) - 1u);
 }
 
+// scipy's binary_dilation with iterations < 1 repeats the dilation until nothing changes: with the
+// 3 x 3 cross over a connected frame that is every pixel as soon as one is set. any_bits_kernel ORs
+// every word into *flag (zeroed first); all_bits_kernel then sets every pixel if it is not zero.
+__global__ void __launch_bounds__(256) any_bits_kernel(const uint32_t *__restrict__ m, int64_t words, uint32_t *flag)
+{
+    uint32_t v = 0;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < words; i += int64_t(gridDim.x) * blockDim.x)
+        v |= m[i];
+    v = __reduce_or_sync(0xffffffffu, v);
+    if ((threadIdx.x & 31) == 0 && v) atomicOr(flag, 1u);
+}
+
+__global__ void __launch_bounds__(256) all_bits_kernel(uint32_t *__restrict__ m, int h, int w, int wpr,
+                                                       const uint32_t *flag)
+{
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= int64_t(h) * wpr || !*flag) return;
+    m[i] = row_bits(int(i % wpr), w);
+}
+
 // mask bits = edge > *thr and sd < max_std, one warp per word (a ballot of its 32 pixels)
 __global__ void __launch_bounds__(256) text_seed_bits_kernel(const float *__restrict__ edge, const float *__restrict__ sd, int h,
                                                              int w, int wpr, const float *__restrict__ thr, float max_std,

@@ -54,7 +54,8 @@ def main(root):
     d = fd(v, chunk=20)
     mask = tm(v, 4, nframes=40, chunk=10)
     mask2 = tm(v, 6, nframes=30, chunk=6, edge_percentile=85, max_std=2.0, dilate=2)
-    np.savez(os.path.join(HERE, 'scans.npz'), frames=v, diff=d, mask=mask, mask2=mask2)
+    mask0 = tm(v, 6, nframes=30, chunk=6, edge_percentile=85, max_std=2.0, dilate=0)   # dilation until no change
+    np.savez(os.path.join(HERE, 'scans.npz'), frames=v, diff=d, mask=mask, mask2=mask2, mask0=mask0)
     print('wrote scans.npz', d.shape, mask.sum(), mask2.sum())
 
 

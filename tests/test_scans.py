@@ -22,6 +22,8 @@ def test_oracle_matches_reference_functions():
     assert np.array_equal(oracle.text_mask(g['frames'], 4, nframes=40, chunk=10), g['mask'])
     assert np.array_equal(oracle.text_mask(g['frames'], 6, nframes=30, chunk=6, edge_percentile=85, max_std=2.0,
                                            dilate=2), g['mask2'])
+    assert np.array_equal(oracle.text_mask(g['frames'], 6, nframes=30, chunk=6, edge_percentile=85, max_std=2.0,
+                                           dilate=0), g['mask0'])
 
 
 @pytest.mark.gpu
@@ -40,6 +42,8 @@ def test_b200_text_mask():
     assert m.dtype == bool and np.array_equal(m, g['mask'])
     m2 = scans.text_mask(g['frames'], 6, nframes=30, chunk=6, edge_percentile=85, max_std=2.0, dilate=2)
     assert np.array_equal(m2, g['mask2'])
+    m0 = scans.text_mask(g['frames'], 6, nframes=30, chunk=6, edge_percentile=85, max_std=2.0, dilate=0)
+    assert np.array_equal(m0, g['mask0'])
 
 
 @pytest.mark.gpu
