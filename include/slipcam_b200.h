@@ -125,7 +125,10 @@ B200_API int b200_correlate_device_surfaces(b200_handle *h, const uint8_t *frame
  * frames go as many per launch as fit), held by every device that loads the library until the
  * process exits; nothing is allocated. Larger frames are rejected with B200_EINVAL. The first call
  * on a device looks the array's address up (cudaGetSymbolAddress): make it before any stream
- * capture. All calls on a device share the array: calls that overlap on the GPU race. */
+ * capture. All calls on a device share the array: calls that overlap on the GPU race.
+ * It always runs the FP32 FFT form, whatever b200_set_form chose for the handle: the tensor-core
+ * and exact-integer forms keep per-launch buffers (spectra, peak records, the refinement queue)
+ * that this entry point has no room for. */
 B200_API int b200_correlate_device_noalloc(b200_handle *h, const uint8_t *frames, int n, int pitch,
                                            const int32_t *gross, int gross_mode, float *offset,
                                            float *peak, float *snr, float *cov, void *stream);

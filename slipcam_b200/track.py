@@ -64,7 +64,7 @@ def track(frames, ref, index, masked=None, window=64, skip=16, search=48, cpu=Fa
           correlator=None):
     """The offsets of the frames index relative to the frame ref, chunk frames per call of the b200
     Correlator; a dict as saved by main (track_offsets.py:35-60). cpu=True is refused: this backend
-    has no CPU path. form: the Correlator's arithmetic ('auto' / 'fft32' / 'tc'). correlator: a
+    has no CPU path. form: the Correlator's arithmetic ('auto' / 'fft32' / 'tc' / 'int8'). correlator: a
     b200 Correlator of this geometry to reuse (its reference is set to frames[ref] here)."""
     if cpu:
         raise ValueError('framecor: the b200 backend has no CPU path (use the reference for cpu=True)')
@@ -100,27 +100,29 @@ def track(frames, ref, index, masked=None, window=64, skip=16, search=48, cpu=Fa
                 out[key][k0:k0 + m] = r[key]
         reader.join()
     elapsed = time.perf_counter() - tic
-    print(f'{len(index)} frames of {ny} x {nx} windows in {elapsed:.1f} s ({elapsed / max(len(index), 1) * 1e3:.1f} ms '
-          f'per frame, framecor {cor.backend}), {masked.sum()} windows masked')
+    per = elapsed / max(len(index), 1) * 1e3
+    print(f'tracked {len(index)} frame(s), {ny * nx} windows each ({ny} rows x {nx} columns): {elapsed:.1f} s, '
+          f'{per:.1f} ms a frame on the {cor.backend} backend; {int(masked.sum())} window(s) under text boxes')
     return dict(index=index, ref=ref, masked=masked, yc=y0 + window / 2, xc=x0 + window / 2, window=window,
                 skip=skip, search=search, engine='framecor', **out)
 
 
 def main(argv=None):
     parser = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
-    parser.add_argument('frames', help='the .npy of the frames (frames x height x width, uint8)')
-    parser.add_argument('--ref', type=int, required=True, help='the reference frame')
-    parser.add_argument('--first', type=int, default=0, help='the first frame (default: %(default)s)')
-    parser.add_argument('--last', type=int, help='the last frame (default: the last of the video)')
-    parser.add_argument('--window', type=int, default=64, help='the window size, pixels (default: %(default)s)')
-    parser.add_argument('--skip', type=int, default=16, help='the distance between windows, pixels (default: %(default)s)')
-    parser.add_argument('--search', type=int, default=48, help='the half search range, pixels (default: %(default)s)')
+    parser.add_argument('frames', help='video as a uint8 .npy array shaped (count, rows, columns)')
+    parser.add_argument('--ref', type=int, required=True, help='index of the frame every other frame is matched to')
+    parser.add_argument('--first', type=int, default=0, help='index of the first tracked frame [%(default)s]')
+    parser.add_argument('--last', type=int, help='index of the last tracked frame, inclusive [end of the video]')
+    parser.add_argument('--window', type=int, default=64, help='side of a square correlation window in px [%(default)s]')
+    parser.add_argument('--skip', type=int, default=16, help='step between neighbouring window origins in px [%(default)s]')
+    parser.add_argument('--search', type=int, default=48, help='largest offset tried in each direction, px [%(default)s]')
     parser.add_argument('--mask', type=int, nargs=4, action='append', default=[], metavar=('X0', 'Y0', 'X1', 'Y1'),
-                        help='a box of burned-in text, pixels (repeatable)')
-    parser.add_argument('--cpu', action='store_true', help='refused: the b200 backend has no CPU path')
-    parser.add_argument('--chunk', type=int, default=64, help='frames per call (default: %(default)s)')
-    parser.add_argument('--form', default='auto', choices=['auto', 'fft32', 'tc'], help='the arithmetic of the transforms')
-    parser.add_argument('--out', required=True, help='the output .npz')
+                        help='pixel box of an overlay (e.g. a timestamp); windows touching it are flagged. May repeat')
+    parser.add_argument('--cpu', action='store_true', help='not available here: this backend runs on the GPU only')
+    parser.add_argument('--chunk', type=int, default=64, help='frames handed to one correlate call [%(default)s]')
+    parser.add_argument('--form', default='auto', choices=['auto', 'fft32', 'tc', 'int8'],
+                        help='correlation arithmetic: auto picks per geometry [%(default)s]')
+    parser.add_argument('--out', required=True, help='where to write the results (.npz)')
     args = parser.parse_args(argv)
 
     frames = np.load(args.frames, mmap_mode='r')
@@ -131,7 +133,7 @@ def main(argv=None):
     result = track(frames, args.ref, np.arange(args.first, last + 1), masked=masked, window=args.window,
                    skip=args.skip, search=args.search, cpu=args.cpu, chunk=args.chunk, form=args.form)
     np.savez(args.out, **result)
-    print(f'-> {args.out}')
+    print(f'wrote {args.out}')
 
 
 if __name__ == '__main__':

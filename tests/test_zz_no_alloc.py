@@ -53,10 +53,13 @@ def test_noalloc_matches_device_entry_point(window, search, skip):
     cor.set_reference(frames[0])
     for first, last in ((1, 6), (6, 12)):
         f, gg = frames[first:last].contiguous(), g[first:last].contiguous()
+        cor.set_form('fft32')
         expect = run('b200_correlate_device', cor, f, gg)
         got = run('b200_correlate_device_noalloc', cor, f, gg)
         same(expect, got)
         assert np.isfinite(got[0]).mean() > 0.9
+        cor.set_form('auto')   # the handle's form does not reach the no-allocation entry point
+        same(expect, run('b200_correlate_device_noalloc', cor, f, gg))
 
 
 def test_noalloc_rejects_frames_too_large():
