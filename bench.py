@@ -9,15 +9,25 @@ search +-48 px), per-frame gross offsets = the rounded camera motion. One step =
 call on a batch of 16 frames (39,200 windows); steps walk through the video.
 
   value       device-timed (CUDA events, max over ranks): frames already in HBM, the device entry
-              point of the C ABI
-  e2e         the host entry point (numpy frames in page-locked host memory -> outputs in numpy
-              arrays), host->device and device->host copies inside the timed region
-  roofline    the fused correlation kernel's achieved FLOP/s (useful FFT work, 2 x 2.5 N^2 log2 N^2
-              + 6 N (N/2+1) per window) over its own CUDA-event time, against the FP32 peak
+              point of the C ABI, in the form chosen by --form (default: the tensor-core form with
+              its exact peak refinement, the library's default at this geometry)
+  e2e         the host entry point with pageable numpy frames (as the reference's callers pass
+              them) -> outputs in numpy arrays, host->device and device->host copies inside the
+              timed region; e2e_pinned the same from page-locked frames
+  roofline    the correlation kernel's achieved rate over its own CUDA-event time, by the unit of
+              work of the form: useful DFT-GEMM FLOPs per window for the tensor-core form (against
+              the measured bf16 tensor peak), useful FFT FLOPs for the FP32 form, 2 W^2 M^2 integer
+              ops for the exact form; traffic from one ncu capture of the same launch
+  accuracy    the timed step's outputs against the exact integer form on the whole step and against
+              the FP64 oracle on a sub-grid
+  other_forms the same step in the other forms
   cpu_baseline the reference's CPU backend (its own sources, FFT by the oracle's shim) on 2 frames
 
 --impl reference: the reference's CPU backend alone (rank 0), one frame per step.
-Multi-GPU (torchrun): each rank correlates its own batches (no collective in the data path).
+--gpus N: each rank correlates its own batches (no collective in the data path); run without a
+launcher, bench.py starts its N ranks itself through torch.distributed.run.
+--workload: the other configurations (mixed grids, 1080p streaming, the differentiable path,
+stabilize, auto_slip's scans), one JSON line each.
 """
 
 import argparse
@@ -100,14 +110,13 @@ class Clocks:
 
 
 # dram bytes per 16-frame launch of the correlation kernel (dram__bytes_read.sum + dram__bytes_write.sum
-# of one ncu capture of this workload; the captures and their commands are summarised in
-# profiles/corr_<form>_720p_w64_s48.md)
+# of one ncu capture of this workload's launch, per form)
 TRAFFIC_PER_LAUNCH = {('fft32', 160): 328990464, ('tc', 160): 377420800}
 
 
 def dft_gemm_flops(n, m):
-    """useful DFT-GEMM work of one window (FFT size n, m shifts per axis), the scope table's formula:
-    forward row real DFT 4 n^2 (n/2+1) + column complex DFT 8 n^2 (n/2+1); inverse pruned to the m
+    """useful DFT-GEMM work of one window (FFT size n, m shifts per axis), one pass at the GEMM form's
+    operand sizes: forward row real DFT 4 n^2 (n/2+1) + column complex DFT 8 n^2 (n/2+1); inverse pruned to the m
     output rows and columns, column 8 m n (n/2+1) + row 4 m^2 (n/2+1) (38.0 MFLOP at n = 160, m = 97)"""
     nh = n // 2 + 1
     return 4 * n * n * nh + 8 * n * n * nh + 8 * m * n * nh + 4 * m * m * nh

@@ -24,8 +24,9 @@
 // second lane tile (searches above 63 px). Rows u >= M, lanes v >= M and chip columns >= L only
 // reach outputs outside the M x M surface, which are never read.
 //
-// Warps: four producers (one per TMEM lane quadrant) fill a ring of stages, one reference row each
-// (every K chunk of both lane tiles, 8 TMEM columns = 128 x 32 bytes per chunk); four epilogue
+// Warps: eight producers (two per TMEM lane quadrant, taking alternate stages) fill a ring of
+// stages, one reference row each (every K chunk of both lane tiles, 8 TMEM columns = 128 x 32 bytes
+// per chunk); four epilogue
 // warps load the next group's chips into shared memory and reduce the previous group's surfaces
 // (normalization, argmax with the reference's tie rule, SNR patch, 3 x 3 fit in FP64); one thread
 // issues the MMAs, one wait and one commit per stage. A group is F frames of one window, so the

@@ -63,6 +63,8 @@ def test_injected_allocation_failure_in_first_call():
             cor.correlate(frames[1:])
     finally:
         _lib.lib().b200_inject_alloc_failure(0)
+    r = cor.correlate(frames[1:])   # nothing was left half-built
+    assert np.isfinite(r['offsets']).mean() > 0.9
 
 
 @pytest.mark.gpu

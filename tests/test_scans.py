@@ -116,15 +116,19 @@ def test_b200_percentile_matches_numpy():
             assert scans.percentile(t, q) == np.percentile(x, q), (x.size, q)
 
 
-def _spiral(h, w):
+def _spiral(h, w, s=4):
+    """Nested rectangular walls s pixels apart, each opened by a gap of s - 1 pixels, at the top
+    left and the bottom right by turns: the background is one corridor that runs half way round
+    every ring (still open after one dilation step, which narrows it to s - 3 pixels)."""
     m = np.zeros((h, w), bool)
     t, l, b, r, k = 2, 2, h - 3, w - 3, 0
-    while t < b and l < r:
-        m[t, l:r + 1] = m[t:b + 1, r] = m[b, l:r + 1] = True
-        m[t + 2:b + 1, l] = True
-        if k % 2:
-            m[t, l + 1] = False
-        t, l, b, r, k = t + 2, l + 2, b - 2, r - 2, k + 1
+    while b - t > s and r - l > s:
+        m[t, l:r + 1] = m[b, l:r + 1] = m[t:b + 1, l] = m[t:b + 1, r] = True
+        if k % 2 == 0:
+            m[t + 1:t + s, l] = False
+        else:
+            m[b - s + 1:b, r] = False
+        t, l, b, r, k = t + s, l + s, b - s, r - s, k + 1
     return m
 
 
@@ -147,8 +151,8 @@ def _mask_device(edge, sd, q, max_std, dilate):
                                  (6, 9000)])
 def test_b200_mask_from_maps_random(h, w):
     """The threshold, dilation and hole filling on the device against the oracle (scipy labels):
-    random seed masks of several densities, dilation 0, 1, 4 and 11 (two launches of the tile
-    dilation), rows of several words per lane in the horizontal sweep (2049 pixels) and wider than
+    random seed masks of several densities, dilation 1, 4 and 11 (two launches of the tile
+    dilation) and 0 (repeated until nothing changes: the whole frame once any pixel is set), rows of several words per lane in the horizontal sweep (2049 pixels) and wider than
     one of its segments (9000 pixels)."""
     rng = np.random.default_rng(h * 1000 + w)
     for dens in (0.02, 0.1, 0.3):
@@ -161,14 +165,15 @@ def test_b200_mask_from_maps_random(h, w):
 
 @pytest.mark.gpu
 def test_b200_mask_fills_spirals_and_rings():
-    """Shapes the sweeps need many rounds for: nested spirals (a corridor that turns at every ring)
-    and a ring inside a ring."""
+    """Shapes the sweeps need many rounds for: nested spirals (a corridor from the border that runs
+    half way round every ring, up to about 4000 pixels long) and a ring inside a ring."""
     for h, w in ((41, 67), (120, 300), (257, 129), (20, 1300)):
         m = _spiral(h, w)
         edge, sd = np.where(m, 100.0, 1.0).astype(np.float32), np.zeros((h, w), np.float32)
         q = 100.0 * (1 - m.mean()) - 1e-3
-        got = _mask_device(edge, sd, q, 1.5, 0)
-        assert np.array_equal(got, oracle.mask_from_maps(edge, sd, q, 1.5, 0))
+        got = _mask_device(edge, sd, q, 1.5, 1)
+        assert not got.all()   # the corridor stays open
+        assert np.array_equal(got, oracle.mask_from_maps(edge, sd, q, 1.5, 1))
     m = np.zeros((90, 140), bool)
     m[5, 5:130] = m[80, 5:130] = True
     m[5:81, 5] = m[5:81, 129] = True
@@ -176,9 +181,9 @@ def test_b200_mask_fills_spirals_and_rings():
     m[20:61, 20] = m[20:61, 99] = True
     m[20, 50] = False   # the inner ring opens into the outer ring's hole: both still enclosed
     edge, sd = np.where(m, 100.0, 1.0).astype(np.float32), np.zeros(m.shape, np.float32)
-    got = _mask_device(edge, sd, 100.0 * (1 - m.mean()) - 1e-3, 1.5, 0)
+    got = _mask_device(edge, sd, 100.0 * (1 - m.mean()) - 1e-3, 1.5, 1)
     assert got[40, 60] and got[70, 60] and not got[2, 2]
-    assert np.array_equal(got, oracle.mask_from_maps(edge, sd, 100.0 * (1 - m.mean()) - 1e-3, 1.5, 0))
+    assert np.array_equal(got, oracle.mask_from_maps(edge, sd, 100.0 * (1 - m.mean()) - 1e-3, 1.5, 1))
 
 
 @pytest.mark.gpu
