@@ -362,7 +362,7 @@ def run_b200(args):
     # the other forms on the same steps (device time), for comparison
     others = {}
     for form in ('fft32', 'tc', 'int8'):
-        if form != args.form:
+        if form != args.form and not args.no_others:
             others[form] = device_rate(form)
     cor.set_form(args.form)
 
@@ -906,6 +906,7 @@ def main():
     p.add_argument('--cpu-frames', type=int, default=2)
     p.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline')
     p.add_argument('--no-e2e', action='store_true', help='device timing only (profiling runs)')
+    p.add_argument('--no-others', action='store_true', help='skip the other forms on the same steps (profiling runs)')
     p.add_argument('--video', type=int, default=NFRAMES, help='frames of the synthetic video to render')
     p.add_argument('--batch', type=int, default=BATCH, help='frames per step')
     p.add_argument('--form', default='tc', choices=['fft32', 'tc', 'int8'], help='the arithmetic of the transforms')

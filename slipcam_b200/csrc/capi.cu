@@ -480,6 +480,7 @@ struct b200_handle {
     DevBuf<float> d_coarse;      // coarse tracking: one frame's surfaces and four outputs
     DevBuf<double> d_cpeaks;     // coarse tracking: one frame's peaks
     cudaEvent_t coarse_ev[6] = {};  // coarse tracking: tables ready (2), tables consumed (2), call start, end
+    std::vector<cudaEvent_t> part_ev;   // host path: a part of a group's frames is on the device
     bool coarse_l2 = false;      // the persisting L2 carve-out for the reference spectra is set up
     cudaAccessPolicyWindow l2win{};   // the window coarse tracking puts on the handle's stream per call
     size_t l2_limit_prev = 0;    // the device's persisting L2 limit before this handle raised it
@@ -503,6 +504,8 @@ struct b200_handle {
             cudaEventDestroy(t.b);
         }
         for (cudaEvent_t e : coarse_ev)
+            if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : part_ev)
             if (e) cudaEventDestroy(e);
         if (l2_raised) cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, l2_limit_prev);   // as it was
         if (comp) cudaStreamDestroy(comp);
@@ -572,12 +575,12 @@ struct b200_handle {
     // beside dinv) serves the exact tensor-core form
     void run_group(const uint8_t *frames, int pitch, int nf, const int32_t *gross, int gross_mode,
                    uint32_t *sat, int64_t *sat2, float *dinv, int2 *bstat, PeakInfo *peaks, int *queue, float *offset,
-                   float *peak, float *snr, float *cov, float *surface, cudaStream_t s)
+                   float *peak, float *snr, float *cov, float *surface, cudaStream_t s, bool tables_done = false)
     {
-        const int arith = form != B200_FORM_I8 ? form : (bstat && ref_u8) ? B200_FORM_I8 : B200_FORM_FFT32;
+        const int arith = group_arith(bstat);
         // the tensor-core form's peaks are refined exactly where the reference windows are at hand
         const bool refine = arith == B200_FORM_TC && peaks && queue && bstat && ref_u8;
-        run_tables(frames, pitch, nf, sat, sat2, dinv, s, arith == B200_FORM_I8 || refine ? bstat : nullptr);
+        if (!tables_done) run_tables(frames, pitch, nf, sat, sat2, dinv, s, wants_bstat(bstat, peaks, queue) ? bstat : nullptr);
         CorrArgs a = corr_args(frames, pitch, nf, gross, gross_mode, sat, dinv, offset, peak, snr, cov, surface);
         a.bstat = bstat;
         a.peaks = refine ? peaks : nullptr;
@@ -604,6 +607,18 @@ struct b200_handle {
             launches += 2;
         }
         launches += 3;
+    }
+
+    // the arithmetic of a launch group: the exact form needs the box table
+    int group_arith(const int2 *bstat) const
+    {
+        return form != B200_FORM_I8 ? form : (bstat && ref_u8) ? B200_FORM_I8 : B200_FORM_FFT32;
+    }
+    // the box table is read by the exact form and by the exact refinement of the tensor-core form
+    bool wants_bstat(const int2 *bstat, const PeakInfo *peaks, const int *queue) const
+    {
+        const int arith = group_arith(bstat);
+        return arith == B200_FORM_I8 || (arith == B200_FORM_TC && peaks && queue && bstat && ref_u8);
     }
 
     // the summed-area tables and the variance denominators of nf frames (and the box table)
@@ -1033,20 +1048,32 @@ int b200_correlate(b200_handle *h, const uint8_t *frames, int n, const int32_t *
                 gbytes = P * 2 * sizeof(int32_t);
                 std::memcpy(s.hgross.p, gross + 2 * size_t(f0) * nwin, gbytes);
             }
-            if (pinned) {
-                CK(cudaMemcpy2DAsync(s.frames.p, h->fpitch, src, h->width, h->width, size_t(nf) * h->height,
-                                     cudaMemcpyHostToDevice, h->copy));
-            } else {
-                // pageable frames: staged into the page-locked slot by the pool, four frames at a time,
-                // each part's DMA issued as soon as it is staged (it runs under the next part's copy)
-                if (!h->pool) h->pool.reset(new CopyPool());
-                for (int c0 = 0; c0 < nf; c0 += 4) {
-                    const int cn = std::min(4, nf - c0);
+            // the frames in parts of four: each part's tables run on the compute stream as soon as the
+            // part is on the device, under the next part's copy (and, for pageable frames, under the
+            // pool's staging of the next part into the page-locked slot)
+            int2 *bst = h->wants_bstat(s.bstat.p, s.peaks.p, s.queue.p) ? s.bstat.p : nullptr;
+            if (!pinned && !h->pool) h->pool.reset(new CopyPool());
+            for (int c0 = 0, part = 0; c0 < nf; c0 += 4, ++part) {
+                const int cn = std::min(4, nf - c0);
+                const uint8_t *from = src + size_t(c0) * frame_bytes;
+                if (!pinned) {   // staged into the page-locked slot (the previous part's DMA runs meanwhile)
                     uint8_t *stage = s.hframes.p + size_t(c0) * frame_bytes;
-                    h->pool->copy(stage, src + size_t(c0) * frame_bytes, size_t(cn) * frame_bytes);
-                    CK(cudaMemcpy2DAsync(s.frames.p + size_t(c0) * h->height * h->fpitch, h->fpitch, stage, h->width,
-                                         h->width, size_t(cn) * h->height, cudaMemcpyHostToDevice, h->copy));
+                    h->pool->copy(stage, from, size_t(cn) * frame_bytes);
+                    from = stage;
                 }
+                uint8_t *dst = s.frames.p + size_t(c0) * h->height * h->fpitch;
+                CK(cudaMemcpy2DAsync(dst, h->fpitch, from, h->width, h->width, size_t(cn) * h->height,
+                                     cudaMemcpyHostToDevice, h->copy));
+                if (int(h->part_ev.size()) <= part) {
+                    cudaEvent_t e = nullptr;
+                    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                    h->part_ev.push_back(e);
+                }
+                CK(cudaEventRecord(h->part_ev[part], h->copy));
+                CK(cudaStreamWaitEvent(h->comp, h->part_ev[part], 0));
+                h->run_tables(dst, h->fpitch, cn, s.sat.p + size_t(c0) * h->sat_size(), s.sat2.p + size_t(c0) * h->sat_size(),
+                              s.dinv.p + size_t(c0) * h->dinv_size(), h->comp,
+                              bst ? bst + size_t(c0) * h->dinv_size() : nullptr);
             }
             if (gbytes) {
                 CK(cudaMemcpyAsync(s.gross.p, s.hgross.p, gbytes, cudaMemcpyHostToDevice, h->copy));
@@ -1056,7 +1083,7 @@ int b200_correlate(b200_handle *h, const uint8_t *frames, int n, const int32_t *
             CK(cudaStreamWaitEvent(h->comp, s.in, 0));
             float *o = s.out.p;
             h->run_group(s.frames.p, h->fpitch, nf, dg, gross_mode, s.sat.p, s.sat2.p, s.dinv.p, s.bstat.p, s.peaks.p, s.queue.p, o, o + 2 * PG,
-                         o + 3 * PG, o + 4 * PG, nullptr, h->comp);
+                         o + 3 * PG, o + 4 * PG, nullptr, h->comp, true);
             CK(cudaMemcpyAsync(s.hout.p, s.out.p, 7 * PG * sizeof(float), cudaMemcpyDeviceToHost, h->comp));
             CK(cudaEventRecord(s.done, h->comp));
         }

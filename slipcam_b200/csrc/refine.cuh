@@ -21,10 +21,17 @@ __host__ __device__ inline int refine_rp(int W) { return (W + 3) & ~3; }
 // the bytes of a staged frame-region row: whole words and one more word for the shifted reads
 __host__ __device__ inline int refine_tp(int nc) { return ((nc + 3) & ~3) + 4; }
 
+// the bytes of a staged region row on the 16-byte path: the row from its aligned 16-byte chunk
+// on (up to 15 bytes before the region), and the words the sums read past it
+__host__ __device__ inline int refine_rt16(int W) { return (4 * (((W + 13) >> 2) + 2) + 15) & ~15; }
+
 // the shared memory of one refinement warp: the reference window and the chip region of the 3 x 3
+// (the larger of the word and 16-byte layouts)
 __host__ __device__ inline size_t refine_warp_smem(int W)
 {
-    return (size_t(W) * refine_rp(W) + size_t(W + 2) * refine_tp(W + 2) + 15) & ~size_t(15);
+    const size_t words = size_t(W) * refine_rp(W) + size_t(W + 2) * refine_tp(W + 2);
+    const size_t b16 = size_t(W) * refine_rp(W) + size_t(W + 2) * refine_rt16(W);
+    return ((words > b16 ? words : b16) + 15) & ~size_t(15);
 }
 
 // the shared memory tc_patch_kernel needs: the reference window and the chip region of the patch
@@ -81,9 +88,28 @@ __device__ __forceinline__ void stage_region(unsigned char *dst, const uint8_t *
     }
 }
 
+// 16 bytes global -> shared without the registers (cp.async, cached in L2 only); the first n of
+// them read, the rest zero
+__device__ __forceinline__ void cp16(unsigned char *dst, const uint8_t *src, int n)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(uint32_t(__cvta_generic_to_shared(dst))),
+                 "l"(src), "r"(n)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// bytes t .. t + 3 (t in 0 .. 5) of the 12 bytes x0 x1 x2 (little-endian)
+__device__ __forceinline__ uint32_t bytes_at(uint32_t x0, uint32_t x1, uint32_t x2, int t)
+{
+    return t < 4 ? __funnelshift_r(x0, x1, 8 * t) : __funnelshift_r(x1, x2, 8 * (t - 4));
+}
+
 // the exact refinement: one warp per pair, its reference window and 3 x 3 chip region staged in
 // the warp's part of the shared memory, the nine sums taken with dp4a (four uint8 products a
-// step), the lanes along the words of the reference rows
+// step), the lanes along the words of the reference rows. When the frame rows start on 16-byte
+// boundaries (and W is a multiple of 4) the staging is 16-byte cp.async copies, many in flight per
+// lane: a region row is copied from its aligned chunk on, the last chunk only up to the frame's
+// width, and the sums read it at the row's byte offset
 __global__ void __launch_bounds__(256) tc_refine_kernel(CorrArgs a, const uint8_t *refwin, const int *sref,
                                                         int *queue)
 {
@@ -106,7 +132,14 @@ __global__ void __launch_bounds__(256) tc_refine_kernel(CorrArgs a, const uint8_
     const int2 *bt0 = a.bstat + size_t(o.f) * a.dinv_fstride + size_t(o.sy) * a.dpitch + o.sx;
     const int sr = sref[k];
     const int wpr = refine_rp(W) / 4;
-    stage_ref(sref_w, ref, W, lane, 32);
+    // the 16-byte path: frame rows on 16-byte boundaries, reference rows of whole words
+    const bool b16 = ((reinterpret_cast<uintptr_t>(a.frames) | uintptr_t(a.pitch) | uintptr_t(a.fstride)) & 15) == 0 &&
+                     (W & 3) == 0;
+    if (b16)
+        for (int e = lane; e < W * W / 16; e += 32) cp16(sref_w + 16 * e, ref + 16 * e, 16);   // W^2 = 16 (W/4)^2
+    else
+        stage_ref(sref_w, ref, W, lane, 32);
+    const int rt = refine_rt16(W);
     int pu = pi.u, pv = pi.v;
     float fit[9];
     int u0 = 0, u1 = 0, v0 = 0, v1 = 0;
@@ -117,21 +150,53 @@ __global__ void __launch_bounds__(256) tc_refine_kernel(CorrArgs a, const uint8_
         v0 = pv > 0 ? -1 : 0;
         v1 = pv < M - 1 ? 1 : 0;
         const int nr = W + u1 - u0, nc = W + v1 - v0, tp = refine_tp(nc);
+        const int c0 = o.sx + pv + v0;   // the region's first frame column
+        const int sh = c0 & 15;          // its byte in the aligned chunk (the same on every row)
         __syncwarp();
-        stage_region(tile, chip + int64_t(pu + u0) * a.pitch + pv + v0, a.pitch, words, nr, nc, lane, 32);
+        if (b16) {
+            // rows of nch chunks from the aligned column c0 - sh; a row's last chunk stops at the
+            // frame's width (the region ends inside the frame, so every chunk starts inside the row)
+            const int nch = (sh + nc + 15) >> 4;
+            const uint8_t *r0 = chip + int64_t(pu + u0) * a.pitch + (pv + v0 - sh);
+            for (int e = lane; e < nr * nch; e += 32) {
+                const int r = e / nch, c = e - r * nch;
+                const int col = c0 - sh + 16 * c;
+                cp16(tile + r * rt + 16 * c, r0 + int64_t(r) * a.pitch + 16 * c, min(16, a.w - col));
+            }
+            cp_wait_all();
+        } else {
+            stage_region(tile, chip + int64_t(pu + u0) * a.pitch + pv + v0, a.pitch, words, nr, nc, lane, 32);
+        }
         __syncwarp();
         uint32_t s[3][3] = {};
-        for (int it = lane; it < W * wpr; it += 32) {
-            const int i = it / wpr, w = it - i * wpr;
-            const uint32_t rw = *reinterpret_cast<const uint32_t *>(sref_w + i * refine_rp(W) + 4 * w);
+        if (b16) {
+            const int sw = sh >> 2, sb = sh & 3;   // the region's first word and byte in a staged row
+            for (int it = lane; it < W * wpr; it += 32) {
+                const int i = it / wpr, w = it - i * wpr;
+                const uint32_t rw = *reinterpret_cast<const uint32_t *>(sref_w + i * W + 4 * w);
 #pragma unroll
-            for (int du = 0; du < 3; ++du) {
-                if (du > u1 - u0) continue;
-                const uint32_t *row = reinterpret_cast<const uint32_t *>(tile + (i + du) * tp) + w;
-                const uint32_t lo = row[0], hi = row[1];
+                for (int du = 0; du < 3; ++du) {
+                    if (du > u1 - u0) continue;
+                    const uint32_t *row = reinterpret_cast<const uint32_t *>(tile + (i + du) * rt) + w + sw;
+                    const uint32_t x0 = row[0], x1 = row[1], x2 = row[2];
 #pragma unroll
-                for (int d = 0; d < 3; ++d)
-                    if (d <= v1 - v0) s[du][d] = __dp4a(rw, d ? __funnelshift_r(lo, hi, 8 * d) : lo, s[du][d]);
+                    for (int d = 0; d < 3; ++d)
+                        if (d <= v1 - v0) s[du][d] = __dp4a(rw, bytes_at(x0, x1, x2, sb + d), s[du][d]);
+                }
+            }
+        } else {
+            for (int it = lane; it < W * wpr; it += 32) {
+                const int i = it / wpr, w = it - i * wpr;
+                const uint32_t rw = *reinterpret_cast<const uint32_t *>(sref_w + i * refine_rp(W) + 4 * w);
+#pragma unroll
+                for (int du = 0; du < 3; ++du) {
+                    if (du > u1 - u0) continue;
+                    const uint32_t *row = reinterpret_cast<const uint32_t *>(tile + (i + du) * tp) + w;
+                    const uint32_t lo = row[0], hi = row[1];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+                        if (d <= v1 - v0) s[du][d] = __dp4a(rw, d ? __funnelshift_r(lo, hi, 8 * d) : lo, s[du][d]);
+                }
             }
         }
 #pragma unroll
