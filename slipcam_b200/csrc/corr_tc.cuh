@@ -236,11 +236,94 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
     // ---- X = chip - round(mean), FP16, K-major (rows i, columns j), zero outside L x L. A warp
     // takes 8 rows x 4 chunks of 8 pixels: 32-byte pieces of 8 rows from global memory, one
     // contiguous 512-byte store into shared memory. Every load of the thread first.
+    // rows16: frame rows on 16-byte boundaries and whole 16-byte chunks per row (the width a
+    // multiple of 16), so a row's chunks never leave it
+    const bool rows16 = ((reinterpret_cast<uintptr_t>(a.frames) | uintptr_t(a.pitch) | uintptr_t(a.fstride)) & 15) == 0 &&
+                        (a.w & 15) == 0;
     auto gather = [&](const PairSetup &c) {
         if (!compute) return;
         const __half2 off = __float2half2_rn(1024.0f + float(c.mean));
         const uint8_t *chip = a.frames + c.f * a.fstride + int64_t(c.sy) * a.pitch + c.sx;
-            {
+        if (rows16 && N <= 160) {
+            // a warp takes groups of 8 chip rows: lane (r, c) = (lane & 7, lane >> 3) loads the aligned
+            // 16-byte chunks c, c + 4, c + 8 of row r (the chip's first byte is byte o of chunk 0, the
+            // same o on every row), then writes chip columns 16 q .. 16 q + 15 (q = c + 4 k) from
+            // chunks q and q + 1 as two 16-byte FP16 pieces: the 8 lanes of one c fill 128
+            // contiguous bytes of a core matrix
+            const int o = c.sx & 15, sw = o >> 2, sb = 8 * (o & 3);
+            const int r = lane & 7, cg = lane >> 3;
+            const int nq = (o + L + 15) >> 4;   // chunks holding chip bytes (they end inside the row)
+            const uint4 *rb = reinterpret_cast<const uint4 *>(chip - o);
+            const int64_t pq = a.pitch >> 4;    // chunks per frame row
+            constexpr int NK = ((N + 30) / 16 + 3) / 4;                  // rounds of 4 chunks (nq <= 4 NK)
+            constexpr int NG = N / 8;                                    // groups of 8 rows
+            constexpr int GPW = (NG + kTcCompute - 1) / kTcCompute;      // groups per warp
+            uint4 all[GPW][NK];   // every load of the warp first: one round trip to memory
+#pragma unroll
+            for (int t = 0; t < GPW; ++t) {
+                const int gi = warp + kTcCompute * t, i = 8 * gi + r;
+#pragma unroll
+                for (int k = 0; k < NK; ++k) {
+                    const int qq = cg + 4 * k;
+                    all[t][k] = make_uint4(0u, 0u, 0u, 0u);
+                    if (gi < NG && i < L && qq < nq) all[t][k] = __ldg(rb + int64_t(i) * pq + qq);
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < GPW; ++t) {
+                const int gi = warp + kTcCompute * t, i = 8 * gi + r;
+                if (gi >= NG) break;   // warp-uniform
+                uint4 raw[NK + 1];
+#pragma unroll
+                for (int k = 0; k < NK; ++k) raw[k] = all[t][k];
+                raw[NK] = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+                for (int k = 0; k < NK; ++k) {
+                    // chunk q + 1: lane (r, c + 1) of this round, or lane (r, 0) of the next
+                    const int down = (lane + 8) & 31;
+                    uint4 nx, nn;
+                    nx.x = __shfl_sync(0xffffffffu, raw[k].x, down);
+                    nx.y = __shfl_sync(0xffffffffu, raw[k].y, down);
+                    nx.z = __shfl_sync(0xffffffffu, raw[k].z, down);
+                    nx.w = __shfl_sync(0xffffffffu, raw[k].w, down);
+                    nn.x = __shfl_sync(0xffffffffu, raw[k + 1].x, r);
+                    nn.y = __shfl_sync(0xffffffffu, raw[k + 1].y, r);
+                    nn.z = __shfl_sync(0xffffffffu, raw[k + 1].z, r);
+                    nn.w = __shfl_sync(0xffffffffu, raw[k + 1].w, r);
+                    if (cg == 3) nx = nn;
+                    const int q = cg + 4 * k;
+                    if (q >= N / 16) continue;
+                    const uint32_t w[8] = {raw[k].x, raw[k].y, raw[k].z, raw[k].w, nx.x, nx.y, nx.z, nx.w};
+                    uint32_t b[5];   // bytes 4 sw .. 4 sw + 19 of the 32 (sw is the same on every lane)
+                    switch (sw) {
+                    case 0: b[0] = w[0]; b[1] = w[1]; b[2] = w[2]; b[3] = w[3]; b[4] = w[4]; break;
+                    case 1: b[0] = w[1]; b[1] = w[2]; b[2] = w[3]; b[3] = w[4]; b[4] = w[5]; break;
+                    case 2: b[0] = w[2]; b[1] = w[3]; b[2] = w[4]; b[3] = w[5]; b[4] = w[6]; break;
+                    default: b[0] = w[3]; b[1] = w[4]; b[2] = w[5]; b[3] = w[6]; b[4] = w[7]; break;
+                    }
+                    uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = make_uint4(0u, 0u, 0u, 0u);
+                    if (i < L) {
+                        bytes_to_half(__funnelshift_r(b[0], b[1], sb), off, lo.x, lo.y);
+                        bytes_to_half(__funnelshift_r(b[1], b[2], sb), off, lo.z, lo.w);
+                        bytes_to_half(__funnelshift_r(b[2], b[3], sb), off, hi.x, hi.y);
+                        bytes_to_half(__funnelshift_r(b[3], b[4], sb), off, hi.z, hi.w);
+                        const int keep = L - 16 * q;   // chip columns from 16 q on
+                        if (keep < 16) {   // the 8 words of the 16 halves: zero past the chip
+                            uint32_t hv[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+#pragma unroll
+                            for (int e = 0; e < 8; ++e) {
+                                if (2 * e >= keep) hv[e] = 0u;
+                                else if (2 * e + 1 >= keep) hv[e] &= 0xFFFFu;
+                            }
+                            lo = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+                            hi = make_uint4(hv[4], hv[5], hv[6], hv[7]);
+                        }
+                    }
+                    *reinterpret_cast<uint4 *>(X + tc::k_major_offset(i, 16 * q, G::SBO_D, 128)) = lo;
+                    *reinterpret_cast<uint4 *>(X + tc::k_major_offset(i, 16 * q + 8, G::SBO_D, 128)) = hi;
+                }
+            }
+        } else {
                 constexpr int NCG = (N / 8 + 3) / 4;               // groups of 4 chunks per row
                 constexpr int NB = (N / 8) * NCG;                   // blocks of 8 rows x 4 chunks
                 constexpr int PERT = (NB + kTcCompute - 1) / kTcCompute;   // blocks per warp
@@ -302,7 +385,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
                     }
                 }
                 }
-            }
+        }
         tc::fence_smem_async();   // the chip is read by the tensor core
     };
 
@@ -427,7 +510,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
         snr_patch(M, a.stat, e_pu, e_pv, i0, i1, j0, j1);
         double sum = 0.0;
         for (int w = 0; w < kTcCompute; ++w) sum += s_sq[w];
-        if (a.peaks) {   // for the exact refinement of the peak (tc_refine_kernel)
+        if (a.peaks) {   // for the exact refinement of the peak, which writes the pair's outputs
             PeakInfo &pi = a.peaks[prev.q];
             pi.valid = 1;
             pi.u = e_pu;
@@ -435,6 +518,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
             pi.count = (i1 - i0) * (j1 - j0);
             pi.sum = sum;
             for (int t = 0; t < 9; ++t) pi.fit[t] = s_fit[t];
+            return;
         }
         peak_outputs(s_fit + 4, 3, M, e_pu, e_pv, R, prev.gy, prev.gx, W * W, sum, (i1 - i0) * (j1 - j0), prev.q,
                      a.offset, a.peak, a.snr, a.cov);
@@ -503,6 +587,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
             failed = true;
             break;
         }
+        // the pending pair's denominators into X (free: S1 has read the chip), under the S1 drain
+        if (prev.live) epi_fetch();
         // S1 -> A2 (MN-major: m = kappa, k = part * N + i); warps w and w + 4 take Re and Im
         for (int t = 0; t < G::T1; ++t) {
             if (!compute || 128 * t + 32 * quad >= N) continue;   // warp-uniform
@@ -521,8 +607,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
         }
         tc_publish();
 
-        // the pending pair's denominators into X (free: S1 has read the chip)
-        if (prev.live) epi_fetch();
         // ---- S2: Z^T = Y^T D: Zr in TMEM columns [0, N), Zi in [N, 2N)
         if (ctrl) {
             B200_TC_DESCS
@@ -537,6 +621,27 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
                 tc::mma_f16(tmem + N, ai, dR0 + 16u * s, id, 1);        // Zi += Yi Dr
             }
             tc::mma_commit(&mbar);
+        }
+        // the next pair's chip and reference spectrum into L2 while the tensor cores run S2 (its
+        // gather comes during this pair's S5, its S3 one pair later): a few prefetches per thread,
+        // every line holding bytes of the chip (inside the frame) or of the window's spectrum
+        if (compute) {
+            const PairSetup &nx = s_next;
+            if (nx.p < npairs && nx.ok) {
+                const uint8_t *chip = a.frames + nx.f * a.fstride + int64_t(nx.sy) * a.pitch + nx.sx;
+                for (int e = tid; e < 3 * L; e += 32 * kTcCompute) {   // a row of L <= 256 bytes spans <= 3 lines
+                    const int i = e / 3, l = e - 3 * i;
+                    const uintptr_t first = reinterpret_cast<uintptr_t>(chip + int64_t(i) * a.pitch);
+                    const uintptr_t line = (first & ~uintptr_t(127)) + 128 * uintptr_t(l);
+                    if (line <= first + uintptr_t(L - 1)) asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
+                }
+                if (nx.k != k) {
+                    const char *r = reinterpret_cast<const char *>(a.spec_tc + size_t(nx.k) * (N / 2) * KP);
+                    constexpr int RL = (N / 2) * KP * 16 / 128;   // whole lines: KP is a multiple of 16
+                    for (int e = tid; e < RL; e += 32 * kTcCompute)
+                        asm volatile("prefetch.global.L2 [%0];" ::"l"(r + 128 * size_t(e)));
+                }
+            }
         }
         // this thread's row of the reference spectrum (S3): frequency pairs (ky, ky + 1) of the
         // rows kappa side by side, KP float4 per pair (rows NH .. KP - 1 zero)
