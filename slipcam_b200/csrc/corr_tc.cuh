@@ -79,11 +79,12 @@ __device__ __forceinline__ uint4 pack8(const float *v)
     return r;
 }
 
-// eight compute warps, two per TMEM lane quadrant (warp w and w + 4 own the same 32 accumulator rows
-// and split their columns), and a control warp whose first thread issues the MMAs and the TMA
-// copies, polls their completion and does the per-pair scalar work, so that no compute warp waits
-// behind the tensor core's issue queue
-constexpr int kTcCompute = 8;
+// kTcCompute compute warps, kTcParts per TMEM lane quadrant (warps w, w + 4, ... own the same 32
+// accumulator rows and split their columns), and a control warp whose first thread issues the MMAs
+// and the TMA copies, polls their completion and does the per-pair scalar work, so that no compute
+// warp waits behind the tensor core's issue queue
+constexpr int kTcCompute = 12;
+constexpr int kTcParts = kTcCompute / 4;
 constexpr int kTcThreads = 32 * (kTcCompute + 1);
 constexpr int kTcCtrl = 32 * kTcCompute;   // the control thread
 
@@ -152,7 +153,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
     __shared__ int s_peak[3];   // the pending pair's peak: valid, u, v
     __shared__ PairSetup s_next;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int quad = warp & 3, half = warp >> 2;
+    const int quad = warp & 3, part = warp >> 2;
     const int row = 32 * quad + lane;   // this thread's accumulator row (TMEM lane)
     const bool compute = warp < kTcCompute, ctrl = tid == kTcCtrl;
     unsigned char *A = smem, *X = smem + G::OFF_X;
@@ -400,7 +401,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
         tma_pending = true;
     };
     // the normalized surface (thread v holds column v) and this thread's argmax; 16-column chunks
-    // of u alternate between the two warps of a quadrant. false if the box did not arrive.
+    // of u alternate among the warps of a quadrant. false if the box did not arrive.
     auto epi_normalize = [&]() -> bool {
         const bool ok = tc::mbar_wait(&tbar, tphase);
         tphase ^= 1u;
@@ -412,7 +413,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
             const bool vin = v < M;
             const float *__restrict__ dv = dvs + (prev.sx & 3) + v;
             float *sv = a.surface ? a.surface + prev.q * M * M + v : nullptr;
-            for (int u0 = 16 * half; u0 < NO; u0 += 32) {   // one 16-column chunk of u per TMEM wait
+            for (int u0 = 16 * part; u0 < NO; u0 += 16 * kTcParts) {   // one 16-column chunk of u per TMEM wait
                 uint32_t cr[16];
                 tc::tmem_ld16_nowait(tmem + lane_base + C5 + uint32_t(u0), cr);
                 const int nu = M - u0 < 16 ? M - u0 : 16;   // rows u of the chunk inside the surface
@@ -469,9 +470,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
         if (e_valid) {
             int i0, i1, j0, j1;
             snr_patch(M, a.stat, e_pu, e_pv, i0, i1, j0, j1);
-            // the warp pair of a quadrant takes alternate 16-row chunks of u from i0
+            // the warps of a quadrant take alternate 16-row chunks of u from i0
             if (compute && 32 * quad < j1 && 32 * quad + 32 > j0) {   // warp-uniform
-                for (int c0 = i0 + 16 * half; c0 < i1; c0 += 32) {
+                for (int c0 = i0 + 16 * part; c0 < i1; c0 += 16 * kTcParts) {
                     const int cb = c0 + 16 <= NO ? c0 : NO - 16;   // 16 columns inside [0, NO)
                     uint32_t cr[16];
                     tc::tmem_ld16_nowait(tmem + lane_base + C5 + uint32_t(cb), cr);
@@ -589,19 +590,21 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
         }
         // the pending pair's denominators into X (free: S1 has read the chip), under the S1 drain
         if (prev.live) epi_fetch();
-        // S1 -> A2 (MN-major: m = kappa, k = part * N + i); warps w and w + 4 take Re and Im
+        // S1 -> A2 (MN-major: m = kappa, k = part * N + i); the warps of a quadrant take the
+        // (Re or Im, column block) units in turn
         for (int t = 0; t < G::T1; ++t) {
             if (!compute || 128 * t + 32 * quad >= N) continue;   // warp-uniform
             const int i = 128 * t + row;
-#pragma unroll
-            for (int cb = 0; cb < KP; cb += 16 * (KP % 32 ? 1 : 2)) {   // 32 (or 16) columns per wait
-                constexpr int NC = KP % 32 ? 16 : 32;
+            constexpr int NC = KP % 32 ? 16 : 32;   // columns per wait
+            constexpr int NCH = KP / NC;
+            for (int un = part; un < 2 * NCH; un += kTcParts) {
+                const int ri = un / NCH, cb = NC * (un - ri * NCH);
                 float v[NC];
-                tc::tmem_ld_cols<NC>(tmem + lane_base + uint32_t(2 * KP * t + half * KP + cb), v);
+                tc::tmem_ld_cols<NC>(tmem + lane_base + uint32_t(2 * KP * t + ri * KP + cb), v);
                 if (i < N) {
 #pragma unroll
                     for (int c0 = 0; c0 < NC; c0 += 8)
-                        *reinterpret_cast<uint4 *>(A + tc::mn_major_offset(cb + c0, half * N + i, G::SBO_A, 128)) = pack8(v + c0);
+                        *reinterpret_cast<uint4 *>(A + tc::mn_major_offset(cb + c0, ri * N + i, G::SBO_A, 128)) = pack8(v + c0);
                 }
             }
         }
@@ -656,23 +659,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
         }
 
         // ---- S3: P = Z conj(R) 2^-(eR + 8) -> A4 (K-major: row kappa, k = part * N + ky); the
-        // 16-column chunks of ky alternate between the two warps of a quadrant
+        // 16-column chunks of ky alternate among the warps of a quadrant
         if (compute && 32 * quad < KP) {
             const float sc = ldexpf(1.0f, -(eR + 8));
-            float4 rn[8];
-#pragma unroll
-            for (int e = 0; e < 8; ++e) rn[e] = kap < KP ? __ldg(rrow + (8 * half + e) * KP) : make_float4(0.f, 0.f, 0.f, 0.f);
-            for (int c0 = 16 * half; c0 < N; c0 += 32) {
+            for (int c0 = 16 * part; c0 < N; c0 += 16 * kTcParts) {
                 uint32_t zr[16], zi[16];
                 tc::tmem_ld16_nowait(tmem + lane_base + uint32_t(c0), zr);
                 tc::tmem_ld16_nowait(tmem + lane_base + uint32_t(N + c0), zi);
-                float4 rc[8];
+                float4 rc[8];   // the spectrum's 16 frequencies of the chunk (the other warps of the quadrant hide the wait)
 #pragma unroll
-                for (int e = 0; e < 8; ++e) rc[e] = rn[e];
-                if (c0 + 32 < N && kap < KP) {
-#pragma unroll
-                    for (int e = 0; e < 8; ++e) rn[e] = __ldg(rrow + ((c0 + 32) / 2 + e) * KP);
-                }
+                for (int e = 0; e < 8; ++e) rc[e] = kap < KP ? __ldg(rrow + (c0 / 2 + e) * KP) : make_float4(0.f, 0.f, 0.f, 0.f);
                 tc::tmem_wait();
                 if (kap < KP) {
 #pragma unroll
@@ -718,14 +714,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
             break;
         }
         // S4 -> B5 in the A region (MN-major: n = u, k = part * KP + kappa), with the Hermitian
-        // weights and 2^-9; warps w and w + 4 take Qr and Qi
+        // weights and 2^-9; the warps of a quadrant take the (Qr or Qi, 32-column block) units in turn
         if (compute && 32 * quad < KP) {
             const int kap = row;
             const float wgt = kap >= NH ? 0.0f : ((kap == 0 || 2 * kap == N) ? 1.0f : 2.0f) * (1.0f / 512.0f);
-            for (int c0 = 0; c0 < NO; c0 += 32) {
+            const int nch = (NO + 31) / 32;
+            for (int un = part; un < 2 * nch; un += kTcParts) {
+                const int reim = un / nch, c0 = 32 * (un - reim * nch);
                 uint32_t r[32];
-                tc::tmem_ld16_nowait(tmem + lane_base + uint32_t(half * NO + c0), r);
-                if (c0 + 16 < NO) tc::tmem_ld16_nowait(tmem + lane_base + uint32_t(half * NO + c0 + 16), r + 16);
+                tc::tmem_ld16_nowait(tmem + lane_base + uint32_t(reim * NO + c0), r);
+                if (c0 + 16 < NO) tc::tmem_ld16_nowait(tmem + lane_base + uint32_t(reim * NO + c0 + 16), r + 16);
                 tc::tmem_wait();
                 if (kap < KP) {
                     float v[32];
@@ -734,7 +732,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
 #pragma unroll
                     for (int h = 0; h < 4; ++h)
                         if (c0 + 8 * h < NO)
-                            *reinterpret_cast<uint4 *>(A + tc::mn_major_offset(c0 + 8 * h, half * KP + kap, G::SBO_B5, 128)) =
+                            *reinterpret_cast<uint4 *>(A + tc::mn_major_offset(c0 + 8 * h, reim * KP + kap, G::SBO_B5, 128)) =
                                 pack8(v + 8 * h, wgt);
                 }
             }
