@@ -582,6 +582,38 @@ def run_stream(args):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     value = steps * batch * nwin / (ms / 1e3)
+
+    # the tensor-core form at this FFT size: the exact integer form (tcgen05 kind::i8, two 128-lane
+    # tiles for the 129 shifts a side) on the same batches; the FP16 DFT-GEMM form does not hold a
+    # 192-point transform beside its operands in shared memory
+    cor.set_form('int8')
+    for i in range(2):
+        cor.correlate(frames[1 + i * batch:1 + (i + 1) * batch])
+    torch.cuda.synchronize()
+    e0.record()
+    for i in range(steps):
+        cor.correlate(frames[1 + i * batch:1 + (i + 1) * batch])
+    e1.record()
+    torch.cuda.synchronize()
+    value_i8 = steps * batch * nwin / (e0.elapsed_time(e1) / 1e3)
+    # both forms against the FP64 oracle on a sample: 2 frames, every 12th row and 16th column of windows
+    from oracle import oracle
+    pick = [1, n // 2]
+    dsub, asub = down[::12], across[::16]
+    o = oracle.correlate(H, W_, dsub, asub, host[0], host[pick], None, window=64, search=64, mode='f64')
+    valid = np.isfinite(o['offsets64'][..., 0])
+    acc = {}
+    for form in ('int8', 'fft32'):
+        cor.set_form(form)
+        rr = cor.correlate(frames[pick])
+        ro = rr['offsets'].cpu().numpy()[:, ::12, ::16]
+        d = np.abs(o['offsets64'] - ro).max(-1)
+        ok = valid & (d <= 0.5)
+        snr = np.abs(rr['snr'].cpu().numpy()[:, ::12, ::16][ok] / o['snr'][ok] - 1)
+        acc[form] = {'pairs': int(valid.sum()), 'max_px': float(d[ok].max()), 'median_px': float(np.median(d[ok])),
+                     'frac_above_0.01px': float((d[ok] > 0.01).mean()), 'integer_peak_mismatches': int((valid & (d > 0.5)).sum()),
+                     'snr_rel_max': float(snr.max())}
+    cor.set_form('fft32')
     t = time.perf_counter()   # the whole job as a user runs it: Correlator, reference spectra, stream
     r = track.track(host, 0, np.arange(1, n + 1), window=64, skip=8, search=64, chunk=batch)
     job_s = time.perf_counter() - t
@@ -602,6 +634,9 @@ def run_stream(args):
         'whole_job': {'value': n * nwin / job_s, 'unit': 'windows/s', 's': job_s,
                       'includes': 'Correlator creation, reference spectra (3.6 GB), the stream'},
         'valid_fraction': float(np.isfinite(r['offsets'][..., 0]).mean()),
+        'other_forms': {'int8': {'value': value_i8, 'unit': 'windows/s',
+                                 'note': 'exact tensor-core form (u8 x u8 -> s32 on tcgen05), the same device batches'}},
+        'accuracy_vs_fp64_oracle': dict(acc, sample=f'frames {pick}, windows rows ::12, columns ::16'),
         'reference_cuda': reference_cuda('stream'),
     }))
 
