@@ -111,7 +111,7 @@ class Clocks:
 
 # dram bytes per 16-frame launch of the correlation kernel (dram__bytes_read.sum + dram__bytes_write.sum
 # of one ncu capture of this workload's launch, per form)
-TRAFFIC_PER_LAUNCH = {('fft32', 160): 328990464, ('tc', 160): 377420800}
+TRAFFIC_PER_LAUNCH = {("fft32", 160): 328990464, ("tc", 160): 380023808}
 
 
 def dft_gemm_flops(n, m):
