@@ -20,6 +20,9 @@
 #include <stdexcept>
 #include <string>
 #include <vector>
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
 
 #include <cudaTypedefs.h>
 
@@ -139,6 +142,37 @@ struct Slot {
 // A pool of host threads that split one large memcpy (pageable caller memory into the page-locked
 // staging slots): one thread copies about 14 GB/s, eight about 40 GB/s. The caller takes a share
 // too and returns when every share is done.
+// n bytes src -> dst with streaming (non-temporal) stores where dst is 16-byte aligned: the
+// page-locked staging buffer is read next by the DMA engine, not by this CPU, and streaming stores
+// skip reading each destination line before writing it. Ends with a store fence, so the bytes are
+// visible to the DMA once the copy is reported done.
+inline void stream_copy(char *dst, const char *src, size_t n)
+{
+#if defined(__SSE2__)
+    size_t i = 0;
+    const size_t head = (16 - (reinterpret_cast<uintptr_t>(dst) & 15)) & 15;
+    if (head) {
+        const size_t m = std::min(head, n);
+        std::memcpy(dst, src, m);
+        i = m;
+    }
+    for (; i + 64 <= n; i += 64) {
+        const __m128i a = _mm_loadu_si128(reinterpret_cast<const __m128i *>(src + i));
+        const __m128i b = _mm_loadu_si128(reinterpret_cast<const __m128i *>(src + i + 16));
+        const __m128i c = _mm_loadu_si128(reinterpret_cast<const __m128i *>(src + i + 32));
+        const __m128i d = _mm_loadu_si128(reinterpret_cast<const __m128i *>(src + i + 48));
+        _mm_stream_si128(reinterpret_cast<__m128i *>(dst + i), a);
+        _mm_stream_si128(reinterpret_cast<__m128i *>(dst + i + 16), b);
+        _mm_stream_si128(reinterpret_cast<__m128i *>(dst + i + 32), c);
+        _mm_stream_si128(reinterpret_cast<__m128i *>(dst + i + 48), d);
+    }
+    if (i < n) std::memcpy(dst + i, src + i, n - i);
+    _mm_sfence();
+#else
+    std::memcpy(dst, src, n);
+#endif
+}
+
 class CopyPool {
   public:
     CopyPool()
@@ -160,7 +194,7 @@ class CopyPool {
     {
         const int parts = int(workers_.size()) + 1;
         if (bytes < (size_t(1) << 20) || parts == 1) {
-            std::memcpy(dst, src, bytes);
+            stream_copy(static_cast<char *>(dst), static_cast<const char *>(src), bytes);
             return;
         }
         const size_t share = (bytes / parts + 4095) & ~size_t(4095);
@@ -175,7 +209,7 @@ class CopyPool {
         }
         cv_.notify_all();
         const size_t o = size_t(parts - 1) * share;   // the caller's share: the last
-        if (o < bytes) std::memcpy(dst_ + o, src_ + o, bytes - o);
+        if (o < bytes) stream_copy(dst_ + o, src_ + o, bytes - o);
         std::unique_lock<std::mutex> lk(m_);
         done_.wait(lk, [this] { return pending_ == 0; });
     }
@@ -193,7 +227,7 @@ class CopyPool {
             const char *sp = src_;
             const size_t o = size_t(i) * share_, n = o < bytes_ ? std::min(share_, bytes_ - o) : 0;
             lk.unlock();
-            if (n) std::memcpy(d + o, sp + o, n);
+            if (n) stream_copy(d + o, sp + o, n);
             lk.lock();
             if (--pending_ == 0) done_.notify_one();
         }
