@@ -169,7 +169,39 @@ __global__ void __launch_bounds__(256) tc_refine_kernel(CorrArgs a, const uint8_
         }
         __syncwarp();
         uint32_t s[3][3] = {};
-        if (b16) {
+        if (b16 && wpr <= 32) {
+            // lane (w, rg) takes word column w of the reference rows ia .. ib - 1 and slides down them
+            // with the three staged region rows of the 3 x 3 in registers: per row one reference word
+            // and one new region row of three words
+            const int sw = sh >> 2, sb = sh & 3;   // the region's first word and byte in a staged row
+            const int nrg = 32 / wpr, rpl = (W + nrg - 1) / nrg;
+            const int w = lane % wpr, rg = lane / wpr;
+            const int ia = rg < nrg ? rg * rpl : W, ib = min(W, ia + rpl);
+            if (ia < ib) {
+                const uint32_t *col = reinterpret_cast<const uint32_t *>(tile) + w + sw;
+                const int rw4 = rt >> 2;   // words per staged row
+                uint32_t a0 = col[ia * rw4], a1 = col[ia * rw4 + 1], a2 = col[ia * rw4 + 2];
+                uint32_t b0 = col[(ia + 1) * rw4], b1 = col[(ia + 1) * rw4 + 1], b2 = col[(ia + 1) * rw4 + 2];
+                for (int i = ia; i < ib; ++i) {
+                    const uint32_t *cr = col + (i + 2) * rw4;   // row i + 2 (inside the W + 2 staged rows)
+                    const uint32_t c0 = cr[0], c1 = cr[1], c2 = cr[2];
+                    const uint32_t rw = *reinterpret_cast<const uint32_t *>(sref_w + i * W + 4 * w);
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        if (d > v1 - v0) continue;
+                        s[0][d] = __dp4a(rw, bytes_at(a0, a1, a2, sb + d), s[0][d]);
+                        if (u1 - u0 >= 1) s[1][d] = __dp4a(rw, bytes_at(b0, b1, b2, sb + d), s[1][d]);
+                        if (u1 - u0 >= 2) s[2][d] = __dp4a(rw, bytes_at(c0, c1, c2, sb + d), s[2][d]);
+                    }
+                    a0 = b0;
+                    a1 = b1;
+                    a2 = b2;
+                    b0 = c0;
+                    b1 = c1;
+                    b2 = c2;
+                }
+            }
+        } else if (b16) {
             const int sw = sh >> 2, sb = sh & 3;   // the region's first word and byte in a staged row
             for (int it = lane; it < W * wpr; it += 32) {
                 const int i = it / wpr, w = it - i * wpr;
