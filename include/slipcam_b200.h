@@ -354,6 +354,12 @@ B200_API int b200_status(b200_handle *h, void *stream, int *status);
  * (injected)"); 0 disables. No counterpart in the reference. */
 B200_API int b200_inject_alloc_failure(int nth);
 
+/* n bytes host memory -> host memory with streaming (non-temporal) stores where dst allows them:
+ * the copy the library stages pageable frames into page-locked buffers with, for callers that stage
+ * frames themselves (the scans and stabilize host paths). Touches no GPU. B200_EINVAL for a null
+ * pointer with n > 0. No reference counterpart. */
+B200_API int b200_host_copy(void *dst, const void *src, size_t n);
+
 /* A check of the bounded waits of the tensor-core kernels, with nothing in flight: one thread waits
  * on an mbarrier that nothing arrives at, with an iteration bound of `polls` and then a clock bound
  * of limit_ms (at most 1000). B200_ETIMEOUT when both waits gave up, as they must; B200_ERUNTIME

@@ -74,6 +74,7 @@ SIGNATURES = {
     'b200_tc_i8_selftest': (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _vp]),
     'b200_status': (_i, [_vp, _vp, ctypes.POINTER(ctypes.c_int)]),
     'b200_inject_alloc_failure': (_i, [_i]),
+    'b200_host_copy': (_i, [_vp, _vp, ctypes.c_size_t]),
     'b200_wait_selftest': (_i, [ctypes.c_uint, ctypes.c_double, _vp]),
     'b200_info': (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i),
                        ctypes.POINTER(ctypes.c_uint64)]),

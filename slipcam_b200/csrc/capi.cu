@@ -562,12 +562,6 @@ struct b200_handle {
             s.sat.alloc(G * sat_size());
             s.sat2.alloc(G * sat_size());
             s.dinv.alloc(G * dinv_size());
-            if (i8_ok) s.bstat.alloc(G * dinv_size());
-            if (i8_ok && tc_ok) {
-                s.peaks.alloc(P);
-                CK(cudaMemset(s.peaks.p, 0, P * sizeof(PeakInfo)));
-                s.queue.alloc(P + 1);
-            }
             s.gross.alloc(2 * P);
             s.out.alloc(7 * P);
             s.hframes.alloc(G * height * fpitch);
@@ -588,20 +582,31 @@ struct b200_handle {
     // by the first device-path call: coarse tracking and the host path never pay for them
     void ensure_tables()
     {
-        if (d_sat.p) return;
-        const size_t G = size_t(group);
-        d_sat.alloc(G * sat_size());
-        d_sat2.alloc(G * sat_size());
-        d_dinv.alloc(G * dinv_size());
-        if (i8_ok) d_bstat.alloc(G * dinv_size());
-        if (i8_ok && tc_ok) {
-            d_peaks.alloc(G * nwin);
-            CK(cudaMemset(d_peaks.p, 0, G * nwin * sizeof(PeakInfo)));
-            d_queue.alloc(G * nwin + 1);
+        if (!d_sat.p) {
+            const size_t G = size_t(group);
+            d_sat.alloc(G * sat_size());
+            d_sat2.alloc(G * sat_size());
+            d_dinv.alloc(G * dinv_size());
+            if (tc_ok) {
+                const CUtensorMap m = dinv_map(d_dinv.p, height, width, dpitch(), int(G), M);
+                CK(cudaMemcpy(d_tmaps.p + 2, &m, sizeof(m), cudaMemcpyHostToDevice));
+            }
         }
-        if (tc_ok) {
-            const CUtensorMap m = dinv_map(d_dinv.p, height, width, dpitch(), int(G), M);
-            CK(cudaMemcpy(d_tmaps.p + 2, &m, sizeof(m), cudaMemcpyHostToDevice));
+        ensure_exact(d_bstat, d_peaks, d_queue);
+    }
+
+    // the exact forms' per-launch buffers, allocated when a form that reads them first runs: the box
+    // table (the exact form, and the exact refinement of the tensor-core form) and the tensor-core
+    // form's peak records and refinement queue (a handle kept on the FP32 form never holds them)
+    void ensure_exact(DevBuf<int2> &bstat, DevBuf<PeakInfo> &peaks, DevBuf<int> &queue)
+    {
+        if (form != B200_FORM_I8 && form != B200_FORM_TC) return;
+        const size_t G = size_t(group), P = G * nwin;
+        if (i8_ok && !bstat.p) bstat.alloc(G * dinv_size());
+        if (i8_ok && tc_ok && !peaks.p) {
+            peaks.alloc(P);
+            CK(cudaMemset(peaks.p, 0, P * sizeof(PeakInfo)));
+            queue.alloc(P + 1);
         }
     }
 
@@ -1049,6 +1054,7 @@ int b200_correlate(b200_handle *h, const uint8_t *frames, int n, const int32_t *
         if (!frames || !offset || !peak || !snr || !cov) fail(B200_EINVAL, "null input or output");
         CK(cudaSetDevice(h->device));
         h->ensure_slots();
+        for (Slot &sl : h->slot) h->ensure_exact(sl.bstat, sl.peaks, sl.queue);
         CK(cudaMemset(h->d_status.p, 0, sizeof(int)));   // a flag left by an earlier call is not this one's
         const int G = h->group, nwin = h->nwin;
         const size_t frame_bytes = size_t(h->height) * h->width;
@@ -1787,6 +1793,14 @@ int b200_inject_alloc_failure(int nth)
 {
     if (nth < 0) return B200_EINVAL;
     g_fail_alloc.store(nth);
+    return B200_OK;
+}
+
+int b200_host_copy(void *dst, const void *src, size_t n)
+{
+    if (n == 0) return B200_OK;
+    if (!dst || !src) return B200_EINVAL;
+    stream_copy(static_cast<char *>(dst), static_cast<const char *>(src), n);
     return B200_OK;
 }
 

@@ -19,6 +19,21 @@ def test_parallel_copy_contiguous_and_strided(shape):
         assert np.array_equal(dst, view)
 
 
+def test_host_copy_any_alignment_and_size():
+    """b200_host_copy (streaming stores past the destination's first 16-byte boundary, plain copies at
+    the ends) moves every byte, at every source and destination offset; no GPU is touched."""
+    from slipcam_b200 import _lib
+    lib = _lib.lib()
+    rng = np.random.default_rng(8)
+    src = rng.integers(0, 256, 1 << 16, dtype=np.uint8)
+    for so, do, n in [(0, 0, 0), (0, 0, 1), (3, 5, 17), (1, 15, 64), (7, 0, 65), (0, 9, 4095), (13, 2, 40000)]:
+        dst = np.zeros(n + 64, np.uint8)
+        assert lib.b200_host_copy(dst.ctypes.data + do, src.ctypes.data + so, n) == _lib.OK
+        assert np.array_equal(dst[do:do + n], src[so:so + n])
+        assert not dst[:do].any() and not dst[do + n:].any()
+    assert lib.b200_host_copy(None, src.ctypes.data, 5) == _lib.EINVAL
+
+
 def test_parallel_copy_from_a_memory_map(tmp_path):
     rng = np.random.default_rng(3)
     a = rng.integers(0, 256, (12, 300, 401), dtype=np.uint8)
