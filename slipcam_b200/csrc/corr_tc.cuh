@@ -234,11 +234,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) corr_tc_kernel(CorrArgs a, cons
         return o;
     };
 
-    // ---- X = chip - round(mean), FP16, K-major (rows i, columns j), zero outside L x L. A warp
-    // takes 8 rows x 4 chunks of 8 pixels: 32-byte pieces of 8 rows from global memory, one
-    // contiguous 512-byte store into shared memory. Every load of the thread first.
-    // rows16: frame rows on 16-byte boundaries and whole 16-byte chunks per row (the width a
-    // multiple of 16), so a row's chunks never leave it
+    // ---- X = chip - round(mean), FP16, K-major (rows i, columns j), zero outside L x L. Two ways:
+    // rows16 (frame rows on 16-byte boundaries and whole 16-byte chunks per row, the width a
+    // multiple of 16, so a row's chunks never leave it): aligned 16-byte chunk loads, below; else a
+    // warp takes 8 rows x 4 chunks of 8 pixels as 4-byte words, 32-byte pieces of 8 rows from global
+    // memory and one contiguous 512-byte store into shared memory. Every load of a thread first.
     const bool rows16 = ((reinterpret_cast<uintptr_t>(a.frames) | uintptr_t(a.pitch) | uintptr_t(a.fstride)) & 15) == 0 &&
                         (a.w & 15) == 0;
     auto gather = [&](const PairSetup &c) {
