@@ -634,9 +634,10 @@ struct b200_handle {
                 CK(cudaFuncSetAttribute(tc_refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
                 attr[dev] = true;
             }
-            // one warp per pair, as many warps per CTA as 96 KB of their tiles hold (at most 8)
+            // one warp per pair, as many warps per CTA as a third of the SM's shared memory holds (at
+            // most 8), so that three CTAs fit on an SM (at window 64: 7 warps of 10.4 KB, 21 per SM)
             const size_t wsm = refine_warp_smem(W);
-            const int wpc = int(std::clamp<size_t>(size_t(96 * 1024) / wsm, 1, 8));
+            const int wpc = int(std::clamp<size_t>(size_t(74 * 1024) / wsm, 1, 8));
             const int64_t pairs = int64_t(nf) * nwin;
             tc_refine_kernel<<<unsigned((pairs + wpc - 1) / wpc), 32 * wpc, size_t(wpc) * wsm, s>>>(a, d_refwin.p, d_sref.p,
                                                                                                    queue);
