@@ -200,6 +200,47 @@ def test_device_equals_host():
         assert np.array_equal(r1[k], r2[k].cpu().numpy(), equal_nan=True), k
 
 
+@pytest.mark.parametrize('form', ['tc', 'int8'])
+@pytest.mark.parametrize('pad', [4, 5])
+def test_rows_off_16_byte_boundaries_give_the_same_outputs(form, pad):
+    """The tensor-core forms read frames whose rows start on 16-byte boundaries with 16-byte chunks
+    (the gather, the refinement's staging) and other frames with 4-byte words or bytes: the same
+    frames, in rows pad bytes off those boundaries (the device entry point with a pitch; the Python
+    device path would make them contiguous), give identical outputs, with per-window gross offsets
+    moving the chips to every byte alignment."""
+    from slipcam_b200 import _lib
+    h, w = 360, 640
+    frames = synth.video(h, w, 4, np.array([[0.0, 0.0], [1.4, -2.6], [-3.1, 0.8], [2.2, 2.9]]), np.zeros(4),
+                         sigma=1.5, noise=1.5, seed=21 + pad)
+    down, across = framecor.window_grid(h, w, 64, 48, 16)
+    cor = framecor.Correlator(h, w, down, across, window=64, search=48, backend='b200')
+    cor.set_form(form)
+    cor.set_reference(frames[0])
+    rng = np.random.default_rng(3 + pad)
+    gross = torch.as_tensor(rng.integers(-9, 10, (3, len(down), len(across), 2)).astype(np.int32)).cuda()
+    t = torch.as_tensor(frames[1:]).cuda()
+    big = torch.zeros((3, h, w + pad), dtype=torch.uint8, device='cuda')
+    big[:, :, pad:] = t
+
+    def run(ptr, pitch):
+        ny, nx = cor.shape
+        out = [torch.empty((3, ny, nx, 2), dtype=torch.float32, device='cuda'),
+               torch.empty((3, ny, nx), dtype=torch.float32, device='cuda'),
+               torch.empty((3, ny, nx), dtype=torch.float32, device='cuda'),
+               torch.empty((3, ny, nx, 3), dtype=torch.float32, device='cuda')]
+        rc = _lib.lib().b200_correlate_device(cor._h, ptr, 3, pitch, gross.data_ptr(), _lib.GROSS_WINDOW,
+                                              *[o.data_ptr() for o in out], torch.cuda.current_stream().cuda_stream)
+        _lib.raise_for(rc, cor._h)
+        return out
+
+    aligned = run(t.data_ptr(), w)
+    off = run(big.data_ptr() + pad, w + pad)
+    for x, y in zip(aligned, off):
+        assert torch.equal(torch.nan_to_num(x, 7.0), torch.nan_to_num(y, 7.0))
+    assert torch.isfinite(aligned[0]).float().mean() > 0.9
+    cor.check()
+
+
 def test_many_groups_host_path():
     """More frames than one launch group: the double-buffered host path keeps every frame's
     outputs in place (the same frames correlated one call at a time agree exactly)."""
