@@ -12,8 +12,9 @@ tensor cores in integers, then normalized.
 * the reference CPU backend's outputs (tests/golden) with the reference test's CPU/CUDA agreement
   bounds;
 * geometries across the kernel's range: odd and tiny windows, searches above 63 px (two lane tiles
-  of shifts), window 128 with search 64 (L = 256), frames that are not 16-byte aligned (the byte
-  gather), several launches of frames.
+  of shifts), window 128 with search 64 (L = 256), several launches of frames (frames in rows off
+  16-byte boundaries, which the Python device path would make contiguous, go through the C entry
+  point with a pitch in test_parity.py).
 """
 
 import numpy as np
@@ -123,7 +124,7 @@ def surfaces_vs_oracle(h, w, window, search, frames, gross=None, skip=24, limit=
     cor.set_form('int8')
     cor.set_reference(frames[0])
     t = torch.as_tensor(frames[1:]).cuda()
-    if pitch_offset:   # frames whose rows do not start on 16-byte boundaries
+    if pitch_offset:   # a strided view (correlate copies it contiguous; the pitch path is in test_parity.py)
         big = torch.zeros((t.shape[0], h, w + pitch_offset), dtype=torch.uint8, device='cuda')
         big[:, :, pitch_offset:] = t
         t = big[:, :, pitch_offset:]
