@@ -634,13 +634,13 @@ struct b200_handle {
                 CK(cudaFuncSetAttribute(tc_refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
                 attr[dev] = true;
             }
-            // one warp per pair, as many warps per CTA as a third of the SM's shared memory holds (at
-            // most 8), so that three CTAs fit on an SM (at window 64: 7 warps of 10.4 KB, 21 per SM)
-            const size_t wsm = refine_warp_smem(W);
-            const int wpc = int(std::clamp<size_t>(size_t(74 * 1024) / wsm, 1, 8));
-            const int64_t pairs = int64_t(nf) * nwin;
-            tc_refine_kernel<<<unsigned((pairs + wpc - 1) / wpc), 32 * wpc, size_t(wpc) * wsm, s>>>(a, d_refwin.p, d_sref.p,
-                                                                                                   queue);
+            // one warp per pair, a CTA per window and up to 8 of its frames (the window staged once),
+            // as many as 100 KB of shared memory holds (at window 64: 8 warps, 55 KB, 4 CTAs an SM)
+            const size_t rsm = refine_ref_smem(W), tsm = refine_tile_smem(W);
+            const int wpc = int(std::clamp<size_t>(std::min<size_t>(size_t(nf), (size_t(100 * 1024) - rsm) / tsm), 1, 8));
+            const int cpw = (nf + wpc - 1) / wpc;
+            tc_refine_kernel<<<unsigned(int64_t(nwin) * cpw), 32 * wpc, rsm + size_t(wpc) * tsm, s>>>(a, d_refwin.p, d_sref.p,
+                                                                                                     queue);
             const size_t psm = tc_patch_smem(W, M, stat);
             tc_patch_kernel<<<unsigned(2 * num_sms()), 256, psm, s>>>(a, d_refwin.p, d_sref.p, queue);
             CK(cudaGetLastError());

@@ -25,12 +25,12 @@ __host__ __device__ inline int refine_tp(int nc) { return ((nc + 3) & ~3) + 4; }
 // on (up to 15 bytes before the region), and the words the sums read past it
 __host__ __device__ inline int refine_rt16(int W) { return (4 * (((W + 13) >> 2) + 2) + 15) & ~15; }
 
-// the shared memory of one refinement warp: the reference window and the chip region of the 3 x 3
-// (the larger of the word and 16-byte layouts)
-__host__ __device__ inline size_t refine_warp_smem(int W)
+// the refinement's shared memory: the CTA's reference window once, then each warp's chip region of
+// its 3 x 3 (the larger of the word and 16-byte layouts)
+__host__ __device__ inline size_t refine_ref_smem(int W) { return (size_t(W) * refine_rp(W) + 15) & ~size_t(15); }
+__host__ __device__ inline size_t refine_tile_smem(int W)
 {
-    const size_t words = size_t(W) * refine_rp(W) + size_t(W + 2) * refine_tp(W + 2);
-    const size_t b16 = size_t(W) * refine_rp(W) + size_t(W + 2) * refine_rt16(W);
+    const size_t words = size_t(W + 2) * refine_tp(W + 2), b16 = size_t(W + 2) * refine_rt16(W);
     return ((words > b16 ? words : b16) + 15) & ~size_t(15);
 }
 
@@ -110,35 +110,42 @@ __device__ __forceinline__ uint32_t bytes_at(uint32_t x0, uint32_t x1, uint32_t 
 // boundaries (and W is a multiple of 4) the staging is 16-byte cp.async copies, many in flight per
 // lane: a region row is copied from its aligned chunk on, the last chunk only up to the frame's
 // width, and the sums read it at the row's byte offset
-__global__ void __launch_bounds__(256) tc_refine_kernel(CorrArgs a, const uint8_t *refwin, const int *sref,
-                                                        int *queue)
+// A CTA takes one window and blockDim / 32 of its frames, a warp per pair: the reference window is
+// staged once for the CTA.
+__global__ void __launch_bounds__(256, 4) tc_refine_kernel(CorrArgs a, const uint8_t *refwin, const int *sref,
+                                                           int *queue)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t p = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;   // the pair (its output index)
-    if (p >= int64_t(a.nwin) * a.nf) return;
-    const PeakInfo &pi = a.peaks[p];
-    const int k = int(p % a.nwin), f = int(p / a.nwin);
-    const i8::Pair o = i8::pair(a, k, f);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int cpw = (a.nf + nw - 1) / nw;   // CTAs per window
+    const int k = blockIdx.x / cpw, f = (blockIdx.x - k * cpw) * nw + warp;
+    if (k >= a.nwin) return;   // the whole CTA
     const int W = a.W, M = a.M, n = W * W;
+    unsigned char *sref_w = smem;
+    const uint8_t *ref = refwin + size_t(k) * W * W;
+    // the 16-byte path: frame rows on 16-byte boundaries, reference rows of whole words
+    const bool b16 = ((reinterpret_cast<uintptr_t>(a.frames) | uintptr_t(a.pitch) | uintptr_t(a.fstride)) & 15) == 0 &&
+                     (W & 3) == 0;
+    if (b16) {
+        for (int e = threadIdx.x; e < W * W / 16; e += blockDim.x) cp16(sref_w + 16 * e, ref + 16 * e, 16);   // W^2 = 16 (W/4)^2
+        cp_wait_all();
+    } else {
+        stage_ref(sref_w, ref, W, threadIdx.x, blockDim.x);
+    }
+    __syncthreads();   // the CTA's one barrier: its warps may leave from here on
+    if (f >= a.nf) return;
+    const int64_t p = int64_t(f) * a.nwin + k;   // the pair (its output index)
+    const PeakInfo &pi = a.peaks[p];
+    const i8::Pair o = i8::pair(a, k, f);
     // only pairs the tensor-core kernel found a peak for (the search window inside the frame)
     if (!o.ok || !pi.valid || pi.u < 0 || pi.u >= M || pi.v < 0 || pi.v >= M) return;
-    unsigned char *sref_w = smem + size_t(warp) * refine_warp_smem(W);
-    unsigned char *tile = sref_w + size_t(W) * refine_rp(W);
+    unsigned char *tile = smem + refine_ref_smem(W) + size_t(warp) * refine_tile_smem(W);
     const uint8_t *chip = a.frames + o.f * a.fstride + int64_t(o.sy) * a.pitch + o.sx;
     const bool words = ((a.pitch | int(a.fstride & 3) | int(reinterpret_cast<uintptr_t>(a.frames) & 3)) & 3) == 0;
-    const uint8_t *ref = refwin + size_t(k) * W * W;
     const float scale = float(1.0 / (double(n) * double(a.norm[k])));
     const int2 *bt0 = a.bstat + size_t(o.f) * a.dinv_fstride + size_t(o.sy) * a.dpitch + o.sx;
     const int sr = sref[k];
     const int wpr = refine_rp(W) / 4;
-    // the 16-byte path: frame rows on 16-byte boundaries, reference rows of whole words
-    const bool b16 = ((reinterpret_cast<uintptr_t>(a.frames) | uintptr_t(a.pitch) | uintptr_t(a.fstride)) & 15) == 0 &&
-                     (W & 3) == 0;
-    if (b16)
-        for (int e = lane; e < W * W / 16; e += 32) cp16(sref_w + 16 * e, ref + 16 * e, 16);   // W^2 = 16 (W/4)^2
-    else
-        stage_ref(sref_w, ref, W, lane, 32);
     const int rt = refine_rt16(W);
     int pu = pi.u, pv = pi.v;
     float fit[9];
