@@ -44,42 +44,35 @@ __global__ void __launch_bounds__(256) sat_rows_kernel(const uint8_t *frames, in
     }
     uint32_t carry = 0;
     int64_t carry2 = 0;
+    // lane l takes pixels x0 + l, x0 + 32 + l, ...: every load and store of the warp is contiguous
     for (int x0 = 0; x0 < w; x0 += 128) {
-        const int xb = x0 + 4 * lane;
-        uint32_t p[4];
-        int64_t p2[4];
-        uint32_t a = 0;
-        int64_t b = 0;
+        uint32_t v[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const uint32_t v = xb + i < w ? row[xb + i] : 0u;
-            a += v;
-            b += int64_t(v * v);
-            p[i] = a;
-            p2[i] = b;
+            const int x = x0 + 32 * i + lane;
+            v[i] = x < w ? uint32_t(__ldg(row + x)) : 0u;
         }
-        // inclusive scan of the lane totals
-        uint32_t sa = a;
-        int64_t sb = b;
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t ta = __shfl_up_sync(0xffffffffu, sa, d);
-            const int64_t tb = __shfl_up_sync(0xffffffffu, sb, d);
-            if (lane >= d) {
-                sa += ta;
-                sb += tb;
+        for (int i = 0; i < 4; ++i) {
+            uint32_t sa = v[i];
+            int64_t sb = int64_t(v[i] * v[i]);
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t ta = __shfl_up_sync(0xffffffffu, sa, d);
+                const int64_t tb = __shfl_up_sync(0xffffffffu, sb, d);
+                if (lane >= d) {
+                    sa += ta;
+                    sb += tb;
+                }
             }
+            const int x = x0 + 32 * i + lane;
+            if (x < w) {
+                o[1 + x] = carry + sa;
+                o2[1 + x] = carry2 + sb;
+            }
+            carry += __shfl_sync(0xffffffffu, sa, 31);
+            carry2 += __shfl_sync(0xffffffffu, sb, 31);
         }
-        const uint32_t ea = carry + sa - a;
-        const int64_t eb = carry2 + sb - b;
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-            if (xb + i < w) {
-                o[1 + xb + i] = ea + p[i];
-                o2[1 + xb + i] = eb + p2[i];
-            }
-        carry += __shfl_sync(0xffffffffu, sa, 31);
-        carry2 += __shfl_sync(0xffffffffu, sb, 31);
     }
 }
 
