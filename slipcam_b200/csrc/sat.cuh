@@ -95,6 +95,7 @@ __global__ void __launch_bounds__(256) sat_cols_kernel(int h, int w, uint32_t *s
             a += s[r * ss + x];
             b += s2[r * ss + x];
         }
+    constexpr int B = 8;   // rows loaded together in the second pass (its stores would otherwise order them)
     c32[ty][tx] = a;
     c64[ty][tx] = b;
     __syncthreads();
@@ -105,11 +106,23 @@ __global__ void __launch_bounds__(256) sat_cols_kernel(int h, int w, uint32_t *s
         cb += c64[t][tx];
     }
     if (x <= w)
-        for (int r = r0; r < r1; ++r) {
-            ca += s[r * ss + x];
-            s[r * ss + x] = ca;
-            cb += s2[r * ss + x];
-            s2[r * ss + x] = cb;
+        for (int rb = r0; rb < r1; rb += B) {
+            uint32_t la[B];
+            long long lb[B];
+#pragma unroll
+            for (int j = 0; j < B; ++j)
+                if (rb + j < r1) {
+                    la[j] = s[(rb + j) * ss + x];
+                    lb[j] = s2[(rb + j) * ss + x];
+                }
+#pragma unroll
+            for (int j = 0; j < B; ++j)
+                if (rb + j < r1) {
+                    ca += la[j];
+                    s[(rb + j) * ss + x] = ca;
+                    cb += lb[j];
+                    s2[(rb + j) * ss + x] = cb;
+                }
         }
 }
 
